@@ -1,0 +1,594 @@
+// gg_api.cu -- the C ABI: context, device memory, and the build/walk pipeline.
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <atomic>
+#include <vector>
+
+#include "gg_internal.cuh"
+#include "gg_kernels.cuh"
+
+#define GG_STACK_CAP 8192
+
+static thread_local char g_last_cuda_error[256];
+
+gg_status gg_cuda_fail(cudaError_t e)
+{
+    snprintf(g_last_cuda_error, sizeof g_last_cuda_error, "%s", cudaGetErrorString(e));
+    cudaGetLastError();   // clear a sticky launch error where possible
+    return e == cudaErrorMemoryAllocation ? GG_ERR_NOMEM : GG_ERR_CUDA;
+}
+
+static std::atomic<long long> g_launches{0};
+void gg_note_launches(int k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+extern "C" int64_t gg_kernel_launches(void) { return (int64_t)g_launches.load(); }
+
+int gg_num_sms()
+{
+    static int cached[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!cached[dev]) {
+        int v = 0;
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        cached[dev] = v > 0 ? v : 148;
+    }
+    return cached[dev];
+}
+
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t cap = 0;
+    gg_status ensure(size_t n)
+    {
+        if (n <= cap && p) return GG_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = n < 1 ? 1 : n;
+        cudaError_t e = cudaMalloc((void **)&p, want * sizeof(T));
+        if (e != cudaSuccess) return gg_cuda_fail(e);
+        cap = want;
+        return GG_OK;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+struct gg_ctx {
+    gg_config cfg;
+    int device = 0;
+    cudaStream_t stream = nullptr, own_stream = nullptr;
+    // systems
+    int S = 0;
+    long long N = 0;
+    std::vector<int> h_poff;
+    bool built = false;
+    // particles
+    DevBuf<int> poff;
+    DevBuf<GGPart> in_rec, part;
+    DevBuf<GGDomainDev> dom;
+    DevBuf<unsigned long long> extent_mm;
+    DevBuf<unsigned long long> keys;
+    DevBuf<unsigned> perm, rank;
+    DevBuf<char> sort_scratch;
+    // tree
+    int ncap = 0;
+    DevBuf<int> t_start, t_end, t_level, t_parent, t_sys, t_nch, t_child, t_counter, t_bnd, t_depth, t_nnodes,
+        t_bsum, t_boff;
+    DevBuf<double> t_mass64;
+    DevBuf<GGNode> nodes;
+    // walk
+    DevBuf<double> oldacc;
+    bool oldacc_valid = false;
+    DevBuf<GGGroup> groups;
+    DevBuf<int> ngroups, gscan, toff, flag, flagscan, tlist, tout, scan_scratch, active_d;
+    DevBuf<int> counters;                  // [0] group counter
+    DevBuf<unsigned long long> inter;      // interaction total
+    DevBuf<int> stack;
+    DevBuf<int> err;
+    DevBuf<double> acc_d, pot_d;
+    DevBuf<int> nint_d;
+    int walk_blocks = 0;
+    // host staging
+    GGPart *h_stage = nullptr;
+    size_t h_stage_cap = 0;
+    // timing
+    cudaEvent_t ev[8];
+    bool have_events = false;
+    gg_stats last;
+};
+
+static gg_status set_device(gg_ctx *c)
+{
+    GG_CUDA_TRY(cudaSetDevice(c->device));
+    return GG_OK;
+}
+
+extern "C" void gg_config_default(gg_config *cfg)
+{
+    memset(cfg, 0, sizeof *cfg);
+    cfg->device = 0;
+    cfg->leaf_size = 8;
+    cfg->group_size = 64;
+    cfg->flush_threshold = 64;
+    cfg->walk_blocks_per_sm = 0;
+    cfg->timing = 0;
+}
+
+extern "C" const char *gg_strerror(gg_status s)
+{
+    switch (s) {
+    case GG_OK: return "ok";
+    case GG_ERR_INVALID: return "invalid argument";
+    case GG_ERR_CUDA: return g_last_cuda_error[0] ? g_last_cuda_error : "CUDA error";
+    case GG_ERR_NOMEM: return "device allocation failed";
+    case GG_ERR_OVERFLOW: return "node pool or walk stack overflow";
+    case GG_ERR_TIMEOUT: return "bounded device wait gave up";
+    case GG_ERR_NOT_BUILT: return "evaluate called before build";
+    case GG_ERR_BAD_INPUT: return "non-finite position, position outside the root cube, or bad index";
+    case GG_ERR_TOO_LARGE: return "size beyond the call's limit";
+    default: return "unknown status";
+    }
+}
+
+extern "C" gg_status gg_create(const gg_config *cfg, gg_ctx **out)
+{
+    if (!out) return GG_ERR_INVALID;
+    *out = nullptr;
+    gg_config c;
+    if (cfg) c = *cfg; else gg_config_default(&c);
+    if (c.leaf_size < 1 || c.leaf_size > 32) return GG_ERR_INVALID;
+    if (c.group_size < 1 || c.group_size > 64) return GG_ERR_INVALID;
+    if (c.flush_threshold < 32 || c.flush_threshold > 128) return GG_ERR_INVALID;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= c.device || c.device < 0) {
+        cudaGetLastError();
+        snprintf(g_last_cuda_error, sizeof g_last_cuda_error, "no CUDA device %d (found %d)", c.device, ndev);
+        return GG_ERR_CUDA;
+    }
+    gg_ctx *ctx = new gg_ctx();
+    ctx->cfg = c;
+    ctx->device = c.device;
+    gg_status st = set_device(ctx);
+    if (st) { delete ctx; return st; }
+    cudaError_t e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete ctx; return gg_cuda_fail(e); }
+    ctx->stream = ctx->own_stream;
+    for (int i = 0; i < 8; i++) cudaEventCreate(&ctx->ev[i]);
+    ctx->have_events = true;
+    memset(&ctx->last, 0, sizeof ctx->last);
+    if ((st = ctx->err.ensure(8)) || (st = ctx->counters.ensure(8)) || (st = ctx->inter.ensure(2))) {
+        gg_destroy(ctx);
+        return st;
+    }
+    cudaMemset(ctx->err.p, 0, 8 * sizeof(int));
+    *out = ctx;
+    return GG_OK;
+}
+
+extern "C" gg_status gg_destroy(gg_ctx *c)
+{
+    if (!c) return GG_ERR_INVALID;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    c->poff.release(); c->in_rec.release(); c->part.release(); c->dom.release(); c->extent_mm.release();
+    c->keys.release(); c->perm.release(); c->rank.release(); c->sort_scratch.release();
+    c->t_start.release(); c->t_end.release(); c->t_level.release(); c->t_parent.release(); c->t_sys.release();
+    c->t_nch.release(); c->t_child.release(); c->t_counter.release(); c->t_bnd.release(); c->t_depth.release();
+    c->t_nnodes.release(); c->t_bsum.release(); c->t_boff.release(); c->t_mass64.release(); c->nodes.release();
+    c->oldacc.release(); c->groups.release(); c->ngroups.release(); c->gscan.release(); c->toff.release();
+    c->flag.release(); c->flagscan.release(); c->tlist.release(); c->tout.release(); c->scan_scratch.release();
+    c->active_d.release(); c->counters.release(); c->inter.release(); c->stack.release(); c->err.release();
+    c->acc_d.release(); c->pot_d.release(); c->nint_d.release();
+    if (c->h_stage) cudaFreeHost(c->h_stage);
+    if (c->have_events)
+        for (int i = 0; i < 8; i++) cudaEventDestroy(c->ev[i]);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return GG_OK;
+}
+
+extern "C" gg_status gg_set_stream(gg_ctx *c, void *s)
+{
+    if (!c) return GG_ERR_INVALID;
+    c->stream = s ? (cudaStream_t)s : c->own_stream;
+    return GG_OK;
+}
+
+extern "C" gg_status gg_synchronize(gg_ctx *c)
+{
+    if (!c) return GG_ERR_INVALID;
+    GG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return GG_OK;
+}
+
+// ---------------------------------------------------------------- particles
+static gg_status set_systems(gg_ctx *c, int S, const int64_t *counts)
+{
+    if (S < 1 || !counts) return GG_ERR_INVALID;
+    long long N = 0;
+    std::vector<int> poff(S + 1);
+    for (int s = 0; s < S; s++) {
+        if (counts[s] < 0) return GG_ERR_INVALID;
+        poff[s] = (int)N;
+        N += counts[s];
+        if (N >= (1ll << 30)) return GG_ERR_TOO_LARGE;
+    }
+    poff[S] = (int)N;
+    c->S = S;
+    c->N = N;
+    c->h_poff = poff;
+    c->built = false;
+    c->oldacc_valid = false;
+    gg_status st;
+    if ((st = c->poff.ensure(S + 1))) return st;
+    GG_CUDA_TRY(cudaMemcpyAsync(c->poff.p, poff.data(), (S + 1) * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    if ((st = c->in_rec.ensure(N)) || (st = c->part.ensure(N)) || (st = c->dom.ensure(S)) ||
+        (st = c->extent_mm.ensure((size_t)S * 6)) || (st = c->keys.ensure(N)) || (st = c->perm.ensure(N)) ||
+        (st = c->rank.ensure(N)) || (st = c->oldacc.ensure(N)))
+        return st;
+    return GG_OK;
+}
+
+extern "C" gg_status gg_load_particles(gg_ctx *c, int32_t S, const int64_t *counts, const double *pos,
+                                       int64_t pos_stride, const double *mass, int64_t mass_stride,
+                                       const double *soft_h, int64_t soft_stride)
+{
+    if (!c || !pos || !mass || !soft_h) return GG_ERR_INVALID;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    if ((st = set_systems(c, S, counts))) return st;
+    if (pos_stride <= 0) pos_stride = 3 * sizeof(double);
+    if (mass_stride <= 0) mass_stride = sizeof(double);
+    if (soft_stride <= 0) soft_stride = sizeof(double);
+    long long N = c->N;
+    if ((size_t)N > c->h_stage_cap) {
+        if (c->h_stage) cudaFreeHost(c->h_stage);
+        c->h_stage = nullptr;
+        c->h_stage_cap = 0;
+        GG_CUDA_TRY(cudaMallocHost((void **)&c->h_stage, (size_t)(N ? N : 1) * sizeof(GGPart)));
+        c->h_stage_cap = (size_t)(N ? N : 1);
+    }
+    GG_CUDA_TRY(cudaStreamSynchronize(c->stream));   // staging buffer may still feed a previous copy
+    const char *pb = (const char *)pos, *mb = (const char *)mass, *hb = (const char *)soft_h;
+    GGPart *dst = c->h_stage;
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < N; i++) {
+        const double *x = (const double *)(pb + i * pos_stride);
+        GGPart r;
+        r.x = x[0]; r.y = x[1]; r.z = x[2];
+        r.m = (float)*(const double *)(mb + i * mass_stride);
+        r.h = (float)*(const double *)(hb + i * soft_stride);
+        dst[i] = r;
+    }
+    if (N) GG_CUDA_TRY(cudaMemcpyAsync(c->in_rec.p, c->h_stage, N * sizeof(GGPart), cudaMemcpyHostToDevice, c->stream));
+    return GG_OK;
+}
+
+extern "C" gg_status gg_load_particles_device(gg_ctx *c, int32_t S, const int64_t *counts, const void *d_records)
+{
+    if (!c || !d_records) return GG_ERR_INVALID;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    if ((st = set_systems(c, S, counts))) return st;
+    if (c->N)
+        GG_CUDA_TRY(cudaMemcpyAsync(c->in_rec.p, d_records, c->N * sizeof(GGPart), cudaMemcpyDeviceToDevice, c->stream));
+    return GG_OK;
+}
+
+// ---------------------------------------------------------------- build
+static int sys_passes(int S)
+{
+    if (S <= 1) return 0;
+    int bits = 0;
+    while ((1 << bits) < S) bits++;
+    return (bits + 7) / 8;
+}
+
+static gg_status ensure_tree(gg_ctx *c)
+{
+    long long cap = 2 * c->N + c->S + 64;
+    if (cap >= (1ll << 31)) return GG_ERR_TOO_LARGE;
+    gg_status st;
+    int G = gg_tree_grid();
+    if ((st = c->t_start.ensure(cap)) || (st = c->t_end.ensure(cap)) || (st = c->t_level.ensure(cap)) ||
+        (st = c->t_parent.ensure(cap)) || (st = c->t_sys.ensure(cap)) || (st = c->t_nch.ensure(cap)) ||
+        (st = c->t_child.ensure(cap)) || (st = c->t_counter.ensure(cap)) || (st = c->t_bnd.ensure(cap * 8)) ||
+        (st = c->t_mass64.ensure(cap)) || (st = c->nodes.ensure(cap)) || (st = c->t_depth.ensure(GG_MAX_DEPTH + 4)) ||
+        (st = c->t_nnodes.ensure(4)) || (st = c->t_bsum.ensure(G + 4)) || (st = c->t_boff.ensure(G + 4)))
+        return st;
+    c->ncap = (int)cap;
+    return GG_OK;
+}
+
+static TreeBuf tree_buf(gg_ctx *c)
+{
+    TreeBuf tb;
+    tb.start = c->t_start.p; tb.end = c->t_end.p; tb.level = c->t_level.p; tb.parent = c->t_parent.p;
+    tb.sys = c->t_sys.p; tb.nch = c->t_nch.p; tb.child = c->t_child.p; tb.counter = c->t_counter.p;
+    tb.bnd = c->t_bnd.p; tb.mass64 = c->t_mass64.p; tb.depth_beg = c->t_depth.p; tb.nnodes = c->t_nnodes.p;
+    tb.blocksum = c->t_bsum.p; tb.blockoff = c->t_boff.p; tb.err = c->err.p;
+    return tb;
+}
+
+extern "C" gg_status gg_build(gg_ctx *c, const gg_domain *domains)
+{
+    if (!c || c->S < 1) return GG_ERR_INVALID;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    cudaStream_t s = c->stream;
+    const int S = c->S, N = (int)c->N;
+    int nsys = sys_passes(S), np = 8 + nsys;
+    if ((st = c->sort_scratch.ensure(gg_sort_scratch_bytes(N, np)))) return st;
+    if ((st = ensure_tree(c))) return st;
+    GG_CUDA_TRY(cudaMemsetAsync(c->err.p, 0, 8 * sizeof(int), s));
+    bool timing = c->cfg.timing != 0;
+    if (timing) cudaEventRecord(c->ev[0], s);
+    if (domains) {
+        std::vector<GGDomainDev> d(S);
+        for (int i = 0; i < S; i++) {
+            for (int k = 0; k < 3; k++) { d[i].center[k] = domains[i].center[k]; d[i].corner[k] = domains[i].corner[k]; }
+            d[i].len = domains[i].len;
+            d[i].pad = 0;
+            if (!(domains[i].len > 0)) return GG_ERR_INVALID;
+        }
+        GG_CUDA_TRY(cudaMemcpyAsync(c->dom.p, d.data(), S * sizeof(GGDomainDev), cudaMemcpyHostToDevice, s));
+        GG_CUDA_TRY(cudaStreamSynchronize(s));
+    } else if (N > 0) {
+        gg_launch_extent(c->in_rec.p, N, c->poff.p, S, c->extent_mm.p, c->dom.p, c->err.p, s);
+    }
+    if (N > 0) gg_launch_keys(c->in_rec.p, N, c->poff.p, S, c->dom.p, c->keys.p, c->perm.p, c->err.p, s);
+    if (timing) cudaEventRecord(c->ev[1], s);
+    if (N > 1) {
+        st = gg_sort_pairs_run(c->keys.p, c->perm.p, N, 8, nsys, c->poff.p, S, c->sort_scratch.p, c->err.p, s);
+        if (st) return st;
+    }
+    if (timing) cudaEventRecord(c->ev[2], s);
+    if (N > 0) gg_launch_permute(c->perm.p, c->in_rec.p, c->part.p, c->rank.p, N, s);
+    gg_launch_tree(c->keys.p, c->poff.p, S, c->cfg.leaf_size, c->ncap, tree_buf(c), c->part.p, c->dom.p, c->nodes.p, s);
+    if (timing) cudaEventRecord(c->ev[3], s);
+    GG_CUDA_TRY(cudaGetLastError());
+    c->built = true;
+    return GG_OK;
+}
+
+extern "C" gg_status gg_get_domains(gg_ctx *c, gg_domain *out)
+{
+    if (!c || !out || c->S < 1) return GG_ERR_INVALID;
+    std::vector<GGDomainDev> d(c->S);
+    GG_CUDA_TRY(cudaMemcpyAsync(d.data(), c->dom.p, c->S * sizeof(GGDomainDev), cudaMemcpyDeviceToHost, c->stream));
+    GG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < c->S; i++) {
+        for (int k = 0; k < 3; k++) { out[i].center[k] = d[i].center[k]; out[i].corner[k] = d[i].corner[k]; }
+        out[i].len = d[i].len;
+    }
+    return GG_OK;
+}
+
+// ---------------------------------------------------------------- walk
+static gg_status walk_setup(gg_ctx *c)
+{
+    gg_status st;
+    if (!c->walk_blocks) {
+        int per_sm = c->cfg.walk_blocks_per_sm;
+        if (per_sm <= 0) per_sm = 2;
+        c->walk_blocks = gg_num_sms() * per_sm;
+    }
+    long long maxg = c->N / c->cfg.group_size + c->S + 1;
+    if ((st = c->groups.ensure(maxg)) || (st = c->ngroups.ensure(2)) || (st = c->gscan.ensure(c->S + 1)) ||
+        (st = c->toff.ensure(c->S + 1)) ||
+        (st = c->stack.ensure((size_t)c->walk_blocks * (gg_walk_threads() / 32) * GG_STACK_CAP)) ||
+        (st = c->scan_scratch.ensure(gg_scan_scratch_ints())))
+        return st;
+    return GG_OK;
+}
+
+// run the walk; outputs to device pointers
+static gg_status run_walk(gg_ctx *c, const int *d_active, int n_active, const double *d_old_acc, double tol,
+                          double theta, double *d_acc, double *d_pot, int *d_nint)
+{
+    gg_status st;
+    cudaStream_t s = c->stream;
+    if ((st = walk_setup(c))) return st;
+    const int S = c->S, N = (int)c->N;
+    const int *tlist = nullptr, *tout = nullptr;
+    const int *toff = c->poff.p;
+    if (d_active) {
+        if ((st = c->flag.ensure(N)) || (st = c->flagscan.ensure(N + 1)) || (st = c->tlist.ensure(N)) ||
+            (st = c->tout.ensure(N)))
+            return st;
+        gg_launch_active(d_active, n_active, c->rank.p, N, c->flag.p, c->flagscan.p, c->tlist.p, c->tout.p, c->poff.p,
+                         S, c->toff.p, c->scan_scratch.p, c->err.p, s);
+        tlist = c->tlist.p;
+        tout = c->tout.p;
+        toff = c->toff.p;
+    }
+    if (d_old_acc) {
+        GG_CUDA_TRY(cudaMemcpyAsync(c->oldacc.p, d_old_acc, (size_t)N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        c->oldacc_valid = true;
+    }
+    gg_launch_groups(toff, S, c->cfg.group_size, c->groups.p, c->ngroups.p, c->gscan.p, s);
+    GG_CUDA_TRY(cudaMemsetAsync(c->counters.p, 0, 8 * sizeof(int), s));
+    GG_CUDA_TRY(cudaMemsetAsync(c->inter.p, 0, 2 * sizeof(unsigned long long), s));
+    WalkParams p;
+    p.nodes = c->nodes.p;
+    p.parts = c->part.p;
+    p.groups = c->groups.p;
+    p.ngroups = c->ngroups.p;
+    p.tlist = tlist;
+    p.tout = tout;
+    p.perm = c->perm.p;
+    p.oldacc_in = c->oldacc_valid ? c->oldacc.p : nullptr;
+    p.oldacc_out = c->oldacc.p;
+    p.tol = tol;
+    p.theta = theta;
+    p.acc = d_acc;
+    p.pot = d_pot;
+    p.ninter = d_nint;
+    p.interactions = c->inter.p;
+    p.group_counter = c->counters.p;
+    p.stack = c->stack.p;
+    p.stack_cap = GG_STACK_CAP;
+    p.err = c->err.p;
+    p.group_size = c->cfg.group_size;
+    p.flush = c->cfg.flush_threshold;
+    int tpl = c->cfg.group_size > 32 ? 2 : 1;
+    if (c->cfg.timing) cudaEventRecord(c->ev[4], s);
+    gg_launch_walk(p, tpl, c->walk_blocks, s);
+    if (c->cfg.timing) cudaEventRecord(c->ev[5], s);
+    c->oldacc_valid = true;
+    GG_CUDA_TRY(cudaGetLastError());
+    return GG_OK;
+}
+
+static gg_status collect_stats(gg_ctx *c, gg_stats *out)
+{
+    int err[8];
+    unsigned long long inter = 0;
+    int nn = 0, ng = 0;
+    GG_CUDA_TRY(cudaMemcpyAsync(err, c->err.p, sizeof err, cudaMemcpyDeviceToHost, c->stream));
+    GG_CUDA_TRY(cudaMemcpyAsync(&inter, c->inter.p, sizeof inter, cudaMemcpyDeviceToHost, c->stream));
+    if (c->t_nnodes.p) GG_CUDA_TRY(cudaMemcpyAsync(&nn, c->t_nnodes.p, sizeof nn, cudaMemcpyDeviceToHost, c->stream));
+    if (c->ngroups.p) GG_CUDA_TRY(cudaMemcpyAsync(&ng, c->ngroups.p, sizeof ng, cudaMemcpyDeviceToHost, c->stream));
+    GG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    gg_stats &L = c->last;
+    L.interactions = (int64_t)inter;
+    L.n_nodes = nn;
+    L.n_groups = ng;
+    L.error_word = err[0];
+    if (c->cfg.timing) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]) == cudaSuccess) L.ms_keys = ms;
+        if (cudaEventElapsedTime(&ms, c->ev[1], c->ev[2]) == cudaSuccess) L.ms_sort = ms;
+        if (cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]) == cudaSuccess) L.ms_build = ms;
+        if (cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]) == cudaSuccess) L.ms_walk = ms;
+        cudaGetLastError();
+    }
+    if (out) *out = L;
+    if (err[0] & GG_EBIT_SORT_TIMEOUT) return GG_ERR_TIMEOUT;
+    if (err[0] & (GG_EBIT_NODE_OVERFLOW | GG_EBIT_STACK_OVERFLOW)) return GG_ERR_OVERFLOW;
+    if (err[0] & GG_EBIT_BAD_INPUT) return GG_ERR_BAD_INPUT;
+    return GG_OK;
+}
+
+extern "C" gg_status gg_last_stats(gg_ctx *c, gg_stats *out)
+{
+    if (!c) return GG_ERR_INVALID;
+    return collect_stats(c, out);
+}
+
+extern "C" gg_status gg_evaluate_device(gg_ctx *c, const int32_t *d_active, int64_t n_active, const double *d_old_acc,
+                                        double tol, double theta, double *d_acc, double *d_pot, int32_t *d_nint)
+{
+    if (!c || !d_acc) return GG_ERR_INVALID;
+    if (!c->built) return GG_ERR_NOT_BUILT;
+    if (d_active && (n_active < 0 || n_active > c->N)) return GG_ERR_INVALID;
+    if (tol < 0 || theta < 0) return GG_ERR_INVALID;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    return run_walk(c, d_active, (int)n_active, d_old_acc, tol, theta, d_acc, d_pot, d_nint);
+}
+
+extern "C" gg_status gg_evaluate(gg_ctx *c, const int32_t *active, int64_t n_active, const double *old_acc,
+                                 double tol, double theta, double *acc_out, double *pot_out, int64_t *ninter_out,
+                                 gg_stats *stats)
+{
+    if (!c || !acc_out) return GG_ERR_INVALID;
+    if (!c->built) return GG_ERR_NOT_BUILT;
+    if (tol < 0 || theta < 0) return GG_ERR_INVALID;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    cudaStream_t s = c->stream;
+    long long nt = active ? n_active : c->N;
+    if (active && (n_active < 0 || n_active > c->N)) return GG_ERR_INVALID;
+    size_t outn = (size_t)(c->N > 0 ? c->N : 1);
+    if ((st = c->acc_d.ensure(outn * 3)) || (st = c->pot_d.ensure(outn)) || (st = c->nint_d.ensure(outn))) return st;
+    const int *d_active = nullptr;
+    if (active) {
+        if ((st = c->active_d.ensure(n_active > 0 ? n_active : 1))) return st;
+        if (n_active)
+            GG_CUDA_TRY(cudaMemcpyAsync(c->active_d.p, active, n_active * sizeof(int), cudaMemcpyHostToDevice, s));
+        d_active = c->active_d.p;
+    }
+    if (old_acc) {
+        GG_CUDA_TRY(cudaMemcpyAsync(c->oldacc.p, old_acc, c->N * sizeof(double), cudaMemcpyHostToDevice, s));
+        c->oldacc_valid = true;
+    }
+    if ((st = run_walk(c, d_active, (int)n_active, nullptr, tol, theta, c->acc_d.p, c->pot_d.p, c->nint_d.p)))
+        return st;
+    if (nt) {
+        GG_CUDA_TRY(cudaMemcpyAsync(acc_out, c->acc_d.p, nt * 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (pot_out) GG_CUDA_TRY(cudaMemcpyAsync(pot_out, c->pot_d.p, nt * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    std::vector<int> ni;
+    if (ninter_out && nt) {
+        ni.resize(nt);
+        GG_CUDA_TRY(cudaMemcpyAsync(ni.data(), c->nint_d.p, nt * sizeof(int), cudaMemcpyDeviceToHost, s));
+    }
+    st = collect_stats(c, stats);
+    if (ninter_out)
+        for (long long i = 0; i < nt; i++) ninter_out[i] = ni[i];
+    c->last.n_targets = nt;
+    if (stats) stats->n_targets = nt;
+    return st;
+}
+
+// ---------------------------------------------------------------- kernel-level entry points
+extern "C" gg_status gg_peano_hilbert_keys(int64_t n, const double *d_pos, const gg_domain *dom, uint64_t *d_keys,
+                                           void *stream)
+{
+    if (n < 0 || !dom || (n && (!d_pos || !d_keys)) || !(dom->len > 0)) return GG_ERR_INVALID;
+    if (n == 0) return GG_OK;
+    GGDomainDev d;
+    for (int k = 0; k < 3; k++) { d.center[k] = dom->center[k]; d.corner[k] = dom->corner[k]; }
+    d.len = dom->len;
+    d.pad = 0;
+    gg_launch_keys_plain(d_pos, n, d, (unsigned long long *)d_keys, nullptr, (cudaStream_t)stream);
+    GG_CUDA_TRY(cudaGetLastError());
+    return GG_OK;
+}
+
+extern "C" gg_status gg_radix_sort_pairs(int64_t n, uint64_t *d_keys, uint32_t *d_vals, int32_t key_bits, void *stream)
+{
+    if (n < 0 || key_bits < 1 || key_bits > 64 || (n && (!d_keys || !d_vals))) return GG_ERR_INVALID;
+    if (n <= 1) return GG_OK;
+    if (n >= (1ll << 30)) return GG_ERR_TOO_LARGE;
+    cudaStream_t s = (cudaStream_t)stream;
+    int np = (key_bits + 7) / 8;
+    size_t bytes = gg_sort_scratch_bytes(n, np);
+    void *scratch = nullptr;
+    int *err = nullptr;
+    GG_CUDA_TRY(cudaMallocAsync(&scratch, bytes, s));
+    cudaError_t e = cudaMallocAsync((void **)&err, 64, s);
+    if (e != cudaSuccess) { cudaFreeAsync(scratch, s); return gg_cuda_fail(e); }
+    cudaMemsetAsync(err, 0, 64, s);
+    gg_status st = gg_sort_pairs_run((unsigned long long *)d_keys, d_vals, n, np, 0, nullptr, 1, scratch, err, s);
+    int herr = 0;
+    cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(scratch, s);
+    cudaFreeAsync(err, s);
+    GG_CUDA_TRY(cudaStreamSynchronize(s));
+    if (st) return st;
+    if (herr & GG_EBIT_SORT_TIMEOUT) return GG_ERR_TIMEOUT;
+    return GG_OK;
+}
+
+extern "C" gg_status gg_direct_sum_fp64(int64_t n_src, const double *d_pos, const double *d_mass, const double *d_h,
+                                        int64_t n_tgt, const int32_t *d_targets, double *d_acc, double *d_pot,
+                                        void *stream)
+{
+    if (n_src < 0 || n_tgt < 0 || (n_src && (!d_pos || !d_mass || !d_h)) || (n_tgt && !d_acc)) return GG_ERR_INVALID;
+    if (!d_targets && n_tgt > n_src) return GG_ERR_INVALID;
+    gg_launch_direct(n_src, d_pos, d_mass, d_h, n_tgt, d_targets, d_acc, d_pot, (cudaStream_t)stream);
+    GG_CUDA_TRY(cudaGetLastError());
+    return GG_OK;
+}

@@ -1,0 +1,71 @@
+// gg_kernels.cuh -- launch functions shared between the kernel files and the API.
+#pragma once
+#include "gg_internal.cuh"
+
+#define GG_SORT_MAX_PASSES 12
+
+// per-node build arrays (device pointers), capacity `cap` nodes
+struct TreeBuf {
+    int *start, *end, *level, *parent, *sys, *nch, *child, *counter;
+    int *bnd;          // 8 digit boundaries per node
+    double *mass64;    // FP64 node mass (parent sums)
+    int *depth_beg;    // GG_MAX_DEPTH + 2 entries
+    int *nnodes;       // total nodes (device)
+    int *blocksum, *blockoff;
+    int *err;
+};
+
+void gg_launch_extent(const GGPart *rec, int n, const int *poff, int S, unsigned long long *mm, GGDomainDev *dom,
+                      int *err, cudaStream_t st);
+void gg_launch_keys(const GGPart *rec, int n, const int *poff, int S, const GGDomainDev *dom,
+                    unsigned long long *keys, unsigned *vals, int *err, cudaStream_t st);
+void gg_launch_keys_plain(const double *pos, long long n, const GGDomainDev &d, unsigned long long *keys, int *err,
+                          cudaStream_t st);
+
+size_t gg_sort_scratch_bytes(long long n, int npasses);
+gg_status gg_sort_pairs_run(unsigned long long *keys, unsigned *vals, long long n, int nkey, int nsys,
+                            const int *poff, int S, void *scratch, int *err, cudaStream_t st);
+
+void gg_launch_permute(const unsigned *perm, const GGPart *in, GGPart *out, unsigned *rank, int n, cudaStream_t st);
+int gg_tree_grid();
+void gg_launch_tree(const unsigned long long *keys, const int *poff, int S, int leaf, int cap, TreeBuf tb,
+                    const GGPart *parts, const GGDomainDev *dom, GGNode *nodes, cudaStream_t st);
+
+struct WalkParams {
+    const GGNode *nodes;
+    const GGPart *parts;        // sorted
+    const GGGroup *groups;
+    const int *ngroups;         // device count
+    const int *tlist;           // sorted particle index per target, NULL = identity
+    const int *tout;            // output slot per target, NULL = load-order index of the particle
+    const unsigned *perm;       // sorted position -> load-order index
+    const double *oldacc_in;    // per particle (load order), NULL = 0
+    double *oldacc_out;         // per particle (load order), may be NULL
+    double tol, theta;
+    double *acc;                // 3 per output slot
+    double *pot;                // per output slot, may be NULL
+    int *ninter;                // per output slot, may be NULL
+    unsigned long long *interactions;
+    int *group_counter;
+    int *stack;
+    int stack_cap;
+    int *err;
+    int group_size;
+    int flush;
+};
+int gg_walk_smem_bytes(int flush, int tpl);
+void gg_launch_walk(const WalkParams &p, int tpl, int blocks, cudaStream_t st);
+int gg_walk_threads();
+
+// groups of `gs` consecutive targets per system; toff[S+1] target offsets per system
+void gg_launch_groups(const int *toff, int S, int gs, GGGroup *groups, int *ngroups, int *gscan, cudaStream_t st);
+// exclusive scan of n ints (scratch: 2 * (gg_num_sms()*4) ints)
+void gg_launch_scan(const int *in, int *out, int n, int *scratch, cudaStream_t st);
+// active targets: flags in sorted order -> tlist/tout, and per-system offsets
+void gg_launch_active(const int *active, int n_active, const unsigned *rank, int n, int *flag, int *flagscan,
+                      int *tlist, int *tout, const int *poff, int S, int *toff, int *scratch, int *err,
+                      cudaStream_t st);
+int gg_scan_scratch_ints();
+
+void gg_launch_direct(long long n_src, const double *pos, const double *mass, const double *h, long long n_tgt,
+                      const int *targets, double *acc, double *pot, cudaStream_t st);

@@ -1,0 +1,305 @@
+// gg_util.cu -- scans, walk-group tables, active-target compaction and the
+// FP64 direct summation used to measure force errors.
+#include "gg_internal.cuh"
+#include "gg_kernels.cuh"
+
+#define SC_THREADS 256
+
+static int scan_blocks() { return gg_num_sms() * 2; }
+int gg_scan_scratch_ints() { return scan_blocks() + 64; }
+
+// ---- exclusive scan of n ints into out[0..n] (out[n] = total); in may be
+// read as 0/1 flags (nonzero_mode) -------------------------------------------
+__device__ __forceinline__ int block_excl_scan(int v, int *ws, int *total)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) ws[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int t = lane < nw ? ws[lane] : 0, u = t;
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, u, o);
+            if (lane >= o) u += y;
+        }
+        if (lane < nw) ws[lane] = u - t;
+        if (lane == nw - 1) ws[32] = u;
+    }
+    __syncthreads();
+    int r = x - v + ws[w];
+    *total = ws[32];
+    __syncthreads();
+    return r;
+}
+
+__global__ void k_scan_reduce(const int *__restrict__ in, int n, int nonzero, int *bsum)
+{
+    __shared__ int ws[33];
+    const int G = gridDim.x, chunk = (n + G - 1) / G;
+    const int cb = blockIdx.x * chunk, ce = min(n, cb + chunk);
+    int acc = 0;
+    for (int i = cb + threadIdx.x; i < ce; i += blockDim.x) {
+        int v = in[i];
+        acc += nonzero ? (v != 0) : v;
+    }
+    int tot;
+    block_excl_scan(acc, ws, &tot);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
+}
+
+__global__ void k_scan_top(int *bsum, int G)
+{
+    __shared__ int ws[33];
+    int carry = 0;
+    for (int base = 0; base < G; base += blockDim.x) {
+        int i = base + threadIdx.x;
+        int v = i < G ? bsum[i] : 0, tot;
+        int e = block_excl_scan(v, ws, &tot);
+        if (i < G) bsum[i] = carry + e;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) bsum[G] = carry;
+}
+
+__global__ void k_scan_down(const int *__restrict__ in, int n, int nonzero, const int *__restrict__ bsum, int *out)
+{
+    __shared__ int ws[33];
+    const int G = gridDim.x, chunk = (n + G - 1) / G;
+    const int cb = blockIdx.x * chunk, ce = min(n, cb + chunk);
+    int run = bsum[blockIdx.x];
+    for (int base = cb; base < ce; base += blockDim.x) {
+        int i = base + threadIdx.x;
+        int v = 0;
+        if (i < ce) { v = in[i]; if (nonzero) v = (v != 0); }
+        int tot;
+        int e = block_excl_scan(v, ws, &tot);
+        if (i < ce) out[i] = run + e;
+        run += tot;
+    }
+    if (blockIdx.x == G - 1 && threadIdx.x == 0) out[n] = bsum[G];
+}
+
+static void scan_run(const int *in, int *out, int n, int nonzero, int *scratch, cudaStream_t st)
+{
+    int G = scan_blocks();
+    k_scan_reduce<<<G, SC_THREADS, 0, st>>>(in, n, nonzero, scratch);
+    k_scan_top<<<1, 1024, 0, st>>>(scratch, G);
+    k_scan_down<<<G, SC_THREADS, 0, st>>>(in, n, nonzero, scratch, out);
+    gg_note_launches(3);
+}
+
+void gg_launch_scan(const int *in, int *out, int n, int *scratch, cudaStream_t st)
+{
+    scan_run(in, out, n, 0, scratch, st);
+}
+
+// ---- groups: ceil(n_s / gs) groups per system -------------------------------
+__global__ void k_groups_count(const int *__restrict__ toff, int S, int gs, int *gscan, int *ngroups)
+{
+    __shared__ int ws[33];
+    int carry = 0;
+    for (int base = 0; base < S; base += blockDim.x) {
+        int s = base + threadIdx.x;
+        int v = 0;
+        if (s < S) v = (toff[s + 1] - toff[s] + gs - 1) / gs;
+        int tot;
+        int e = block_excl_scan(v, ws, &tot);
+        if (s < S) gscan[s] = carry + e;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) {
+        gscan[S] = carry;
+        *ngroups = carry;
+    }
+}
+
+__global__ void k_groups_write(const int *__restrict__ toff, const int *__restrict__ gscan, int S, int gs,
+                               const int *__restrict__ ngroups, GGGroup *groups)
+{
+    const int ng = *ngroups;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+        int lo = 0, hi = S - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (gscan[mid] <= g) lo = mid; else hi = mid - 1;
+        }
+        int s = lo;
+        int k = g - gscan[s];
+        int first = toff[s] + k * gs;
+        GGGroup gr;
+        gr.first = first;
+        gr.count = min(gs, toff[s + 1] - first);
+        gr.root = s;
+        gr.sys = s;
+        groups[g] = gr;
+    }
+}
+
+void gg_launch_groups(const int *toff, int S, int gs, GGGroup *groups, int *ngroups, int *gscan, cudaStream_t st)
+{
+    k_groups_count<<<1, 1024, 0, st>>>(toff, S, gs, gscan, ngroups);
+    k_groups_write<<<gg_num_sms() * 8, 256, 0, st>>>(toff, gscan, S, gs, ngroups, groups);
+    gg_note_launches(2);
+}
+
+// ---- active targets ------------------------------------------------------------
+__global__ void k_mark_active(const int *__restrict__ active, int n_active, const unsigned *__restrict__ rank, int n,
+                              int *flag, int *err)
+{
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n_active; j += gridDim.x * blockDim.x) {
+        int a = active[j];
+        if (a < 0 || a >= n) { atomicOr(err, GG_EBIT_BAD_INPUT); continue; }
+        flag[rank[a]] = j + 1;
+    }
+}
+
+__global__ void k_compact_active(const int *__restrict__ flag, const int *__restrict__ scan, int n, int *tlist,
+                                 int *tout, const int *__restrict__ poff, int S, int *toff)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int f = flag[i];
+        if (f) {
+            int t = scan[i];
+            tlist[t] = i;
+            tout[t] = f - 1;
+        }
+    }
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s <= S; s += gridDim.x * blockDim.x) toff[s] = scan[poff[s]];
+}
+
+void gg_launch_active(const int *active, int n_active, const unsigned *rank, int n, int *flag, int *flagscan,
+                      int *tlist, int *tout, const int *poff, int S, int *toff, int *scratch, int *err,
+                      cudaStream_t st)
+{
+    cudaMemsetAsync(flag, 0, (size_t)n * sizeof(int), st);
+    k_mark_active<<<gg_num_sms() * 4, 256, 0, st>>>(active, n_active, rank, n, flag, err);
+    scan_run(flag, flagscan, n, 1, scratch, st);
+    k_compact_active<<<gg_num_sms() * 8, 256, 0, st>>>(flag, flagscan, n, tlist, tout, poff, S, toff);
+    gg_note_launches(2);
+}
+
+// ---- FP64 direct summation ---------------------------------------------------
+// Same pair rule as the walk (forcetree.c:2258-2283): Newtonian when r >= h_i
+// and r >= h_j, otherwise the cubic spline with h = max(h_i, h_j).
+__device__ __forceinline__ void spline64(double u, double hinv, double *wf, double *wp)
+{
+    if (u < 0.5) {
+        *wf = (10.666666666667 + u * u * (32.0 * u - 38.4)) * hinv * hinv * hinv;
+        *wp = (-2.8 + u * u * (5.333333333333 + u * u * (6.4 * u - 9.6))) * hinv;
+    } else {
+        *wf = (21.333333333333 - 48.0 * u + 38.4 * u * u - 10.666666666667 * u * u * u - 0.066666666667 / (u * u * u)) *
+              hinv * hinv * hinv;
+        *wp = (-3.2 + 0.066666666667 / u + u * u * (10.666666666667 + u * (-16.0 + u * (9.6 - 2.133333333333 * u)))) *
+              hinv;
+    }
+}
+
+#define DS_TILE 256
+__global__ void __launch_bounds__(DS_TILE) k_direct(long long nsrc, const double *__restrict__ pos,
+                                                    const double *__restrict__ mass, const double *__restrict__ h,
+                                                    long long ntgt, const int *__restrict__ targets, double *acc,
+                                                    double *pot)
+{
+    __shared__ double sx[DS_TILE], sy[DS_TILE], sz[DS_TILE], sm[DS_TILE], sh[DS_TILE];
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    bool valid = t < ntgt;
+    long long i = valid ? (targets ? targets[t] : t) : 0;
+    double xi = pos[3 * i], yi = pos[3 * i + 1], zi = pos[3 * i + 2], hi = h[i];
+    double ax = 0, ay = 0, az = 0, pp = 0;
+    for (long long base = 0; base < nsrc; base += DS_TILE) {
+        long long j = base + threadIdx.x;
+        __syncthreads();
+        if (j < nsrc) {
+            sx[threadIdx.x] = pos[3 * j]; sy[threadIdx.x] = pos[3 * j + 1]; sz[threadIdx.x] = pos[3 * j + 2];
+            sm[threadIdx.x] = mass[j]; sh[threadIdx.x] = h[j];
+        } else {
+            sm[threadIdx.x] = 0; sx[threadIdx.x] = sy[threadIdx.x] = sz[threadIdx.x] = 0; sh[threadIdx.x] = 0;
+        }
+        __syncthreads();
+        int m = (int)min((long long)DS_TILE, nsrc - base);
+        for (int k = 0; k < m; k++) {
+            double dx = sx[k] - xi, dy = sy[k] - yi, dz = sz[k] - zi;
+            double r2 = dx * dx + dy * dy + dz * dz;
+            double mj = sm[k];
+            if (r2 > 0 && mj > 0) {
+                double r = sqrt(r2), hj = sh[k], fac, fp;
+                if (r >= hi && r >= hj) {
+                    fac = mj / (r2 * r);
+                    fp = -mj / r;
+                } else {
+                    double hg = hi > hj ? hi : hj, hinv = 1.0 / hg, wf, wp;
+                    spline64(r * hinv, hinv, &wf, &wp);
+                    fac = mj * wf;
+                    fp = mj * wp;
+                }
+                ax += dx * fac; ay += dy * fac; az += dz * fac; pp += fp;
+            }
+        }
+    }
+    if (valid) {
+        acc[3 * t] = ax; acc[3 * t + 1] = ay; acc[3 * t + 2] = az;
+        if (pot) pot[t] = pp;
+    }
+}
+
+void gg_launch_direct(long long n_src, const double *pos, const double *mass, const double *h, long long n_tgt,
+                      const int *targets, double *acc, double *pot, cudaStream_t st)
+{
+    long long blocks = (n_tgt + DS_TILE - 1) / DS_TILE;
+    if (blocks < 1) return;
+    k_direct<<<(unsigned)blocks, DS_TILE, 0, st>>>(n_src, pos, mass, h, n_tgt, targets, acc, pot);
+    gg_note_launches(1);
+}
+
+// ---- FP32 FMA throughput probe ---------------------------------------------
+// Independent FMA chains per thread, enough warps to fill every SM: the
+// CUDA-core FP32 roofline that the walk is measured against.
+#define PEAK_CHAINS 8
+__global__ void k_fma_peak(float *out, int iters, float a, float b)
+{
+    float x[PEAK_CHAINS];
+#pragma unroll
+    for (int c = 0; c < PEAK_CHAINS; c++) x[c] = threadIdx.x * 1e-7f + c;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int c = 0; c < PEAK_CHAINS; c++) x[c] = fmaf(x[c], a, b);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int c = 0; c < PEAK_CHAINS; c++) s += x[c];
+    if (s == 1234.5f) out[0] = s;   // keeps the chains live
+}
+
+extern "C" gg_status gg_fp32_peak_probe(double *tflops, void *stream)
+{
+    if (!tflops) return GG_ERR_INVALID;
+    cudaStream_t st = (cudaStream_t)stream;
+    float *out = nullptr;
+    GG_CUDA_TRY(cudaMallocAsync((void **)&out, 64, st));
+    const int threads = 512, blocks = gg_num_sms() * 4, iters = 1 << 14;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best = 0;
+    for (int rep = 0; rep < 4; rep++) {
+        cudaEventRecord(e0, st);
+        k_fma_peak<<<blocks, threads, 0, st>>>(out, iters, 0.999999f, 1e-7f);
+        gg_note_launches(1);
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        double fl = 2.0 * PEAK_CHAINS * (double)iters * threads * blocks;
+        if (ms > 0 && rep > 0) best = fl / (ms * 1e-3) / 1e12 > best ? fl / (ms * 1e-3) / 1e12 : best;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFreeAsync(out, st);
+    GG_CUDA_TRY(cudaStreamSynchronize(st));
+    *tflops = best;
+    return GG_OK;
+}

@@ -1,0 +1,454 @@
+// gg_walk.cu -- warp-cooperative tree walk (force_treeevaluate, forcetree.c:1633-2807).
+//
+// A warp serves one group of up to 32*TPL targets that are consecutive in
+// Peano-Hilbert order (TPL targets per lane).  The warp walks the tree once
+// for the whole group with an explicit node stack: each round pops up to 32
+// nodes, one per lane, and tests them against the group's bounding box with
+// the reference's opening rules made conservative over the group
+// (distance = from the node's centre of mass to the box, the smallest
+// ErrTolForceAcc*OldAcc of the group, the largest target softening):
+//   - massless nodes are skipped                         (forcetree.c:2038)
+//   - one-particle nodes are always opened               (:2043-2050)
+//   - h < maxsoft and r^2 < maxsoft^2 opens              (:2099-2102)
+//   - Barnes-Hut pass: len^2 > r^2 theta^2 opens         (:2104-2111)
+//   - relative pass: r^2 < (soft+0.6 len)^2 or
+//     r^2 < (maxsoft+0.6 len)^2, m len^2 > r^4 aold, or
+//     the target inside the 1.2*len box opens           (:2119-2147)
+// For a group of one target these are exactly the reference's tests.  Tests
+// run in FP64 on the FP64 centre of mass.  Used nodes and particles are
+// appended (ballot + popc compaction) to per-warp shared-memory lists as
+// FP32 offsets from the group centre; a "far" list holds entries that are
+// Newtonian for every target of the group (no softening branch, no self
+// term) and a "near" list holds the rest.  When a list reaches the flush
+// threshold every lane evaluates it for its targets in FP32 (cubic-spline
+// softening, kernel.h:452-470, with h = max(h_target, h_source),
+// forcetree.c:2263-2283); each flush's partial sums are added to the
+// per-target totals with Kahan compensation.  Interactions are counted like
+// the reference (forcetree.c:2258, :2488): one per used node or particle with
+// r^2 > 0 and m > 0.
+#include "gg_internal.cuh"
+#include "gg_kernels.cuh"
+
+#define WALK_THREADS 256
+#define WALK_WARPS (WALK_THREADS / 32)
+#define FULL 0xffffffffu
+
+int gg_walk_threads() { return WALK_THREADS; }
+
+int gg_walk_smem_bytes(int flush, int tpl)
+{
+    (void)tpl;
+    int cap = flush + 32;
+    // per warp: far float4[cap], near float4[cap], near h float[cap] (rounded up to float4)
+    return WALK_WARPS * (2 * cap + cap / 4 + 1) * 16;
+}
+
+__device__ __forceinline__ GGNode load_node(const GGNode *p)
+{
+    GGNode r;
+    const int4 *src = reinterpret_cast<const int4 *>(p);
+    int4 *dst = reinterpret_cast<int4 *>(&r);
+#pragma unroll
+    for (int i = 0; i < 4; i++) dst[i] = __ldg(src + i);
+    return r;
+}
+
+__device__ __forceinline__ GGPart load_part(const GGPart *p)
+{
+    GGPart r;
+    const int4 *src = reinterpret_cast<const int4 *>(p);
+    int4 *dst = reinterpret_cast<int4 *>(&r);
+    dst[0] = __ldg(src);
+    dst[1] = __ldg(src + 1);
+    return r;
+}
+
+struct Kahan {
+    float s, c;
+    __device__ __forceinline__ void add(float x)
+    {
+        float y = x - c;
+        float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
+
+// cubic-spline softened force and potential factors for u = r/h < 1
+// (kernel.h:452-470); returns w_force, writes w_pot; both still to be scaled
+// by hinv^3 and hinv.
+__device__ __forceinline__ float spline_wf(float u, float *wp)
+{
+    float u2 = u * u;
+    if (u < 0.5f) {
+        *wp = -2.8f + u2 * (5.333333333333f + u2 * (6.4f * u - 9.6f));
+        return 10.666666666667f + u2 * (32.0f * u - 38.4f);
+    }
+    float iu = 1.0f / u;
+    *wp = -3.2f + 0.066666666667f * iu + u2 * (10.666666666667f + u * (-16.0f + u * (9.6f - 2.133333333333f * u)));
+    return 21.333333333333f - 48.0f * u + 38.4f * u2 - 10.666666666667f * u2 * u - 0.066666666667f * iu * iu * iu;
+}
+
+template <int TPL>
+struct Targets {
+    float x[TPL], y[TPL], z[TPL], h[TPL];
+    bool valid[TPL];
+    Kahan ax[TPL], ay[TPL], az[TPL], pot[TPL];
+    int nint[TPL];
+};
+
+template <int TPL>
+__device__ __forceinline__ void flush_far(const float4 *__restrict__ far, int nf, Targets<TPL> &T)
+{
+    __syncwarp();
+    float px[TPL], py[TPL], pz[TPL], pp[TPL];
+#pragma unroll
+    for (int s = 0; s < TPL; s++) { px[s] = 0.f; py[s] = 0.f; pz[s] = 0.f; pp[s] = 0.f; }
+#pragma unroll 4
+    for (int j = 0; j < nf; j++) {
+        const float4 e = far[j];
+#pragma unroll
+        for (int s = 0; s < TPL; s++) {
+            float dx = e.x - T.x[s], dy = e.y - T.y[s], dz = e.z - T.z[s];
+            float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            float rinv = rsqrtf(r2);
+            float mr = e.w * rinv;
+            float fac = mr * rinv * rinv;
+            px[s] = fmaf(dx, fac, px[s]);
+            py[s] = fmaf(dy, fac, py[s]);
+            pz[s] = fmaf(dz, fac, pz[s]);
+            pp[s] -= mr;
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < TPL; s++) {
+        T.ax[s].add(px[s]); T.ay[s].add(py[s]); T.az[s].add(pz[s]); T.pot[s].add(pp[s]);
+        T.nint[s] += nf;
+    }
+    __syncwarp();
+}
+
+template <int TPL>
+__device__ __forceinline__ void flush_near(const float4 *__restrict__ nearE, const float *__restrict__ nearH, int nn,
+                                           Targets<TPL> &T)
+{
+    __syncwarp();
+    float px[TPL], py[TPL], pz[TPL], pp[TPL];
+#pragma unroll
+    for (int s = 0; s < TPL; s++) { px[s] = 0.f; py[s] = 0.f; pz[s] = 0.f; pp[s] = 0.f; }
+    for (int j = 0; j < nn; j++) {
+        const float4 e = nearE[j];
+        const float hp = nearH[j];
+#pragma unroll
+        for (int s = 0; s < TPL; s++) {
+            float dx = e.x - T.x[s], dy = e.y - T.y[s], dz = e.z - T.z[s];
+            float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            if (r2 > 0.f) {
+                float hg = fmaxf(T.h[s], hp);
+                float rinv = rsqrtf(r2);
+                float fac, fpot;
+                if (r2 >= hg * hg) {
+                    float mr = e.w * rinv;
+                    fac = mr * rinv * rinv;
+                    fpot = -mr;
+                } else {
+                    float hinv = 1.0f / hg;
+                    float u = r2 * rinv * hinv;
+                    float wp;
+                    float wf = spline_wf(u, &wp);
+                    fac = e.w * wf * hinv * hinv * hinv;
+                    fpot = e.w * wp * hinv;
+                }
+                px[s] = fmaf(dx, fac, px[s]);
+                py[s] = fmaf(dy, fac, py[s]);
+                pz[s] = fmaf(dz, fac, pz[s]);
+                pp[s] += fpot;
+                T.nint[s] += 1;
+            }
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < TPL; s++) {
+        T.ax[s].add(px[s]); T.ay[s].add(py[s]); T.az[s].add(pz[s]); T.pot[s].add(pp[s]);
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ double warp_min_d(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(FULL, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_max_d(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(FULL, v, o));
+    return v;
+}
+__device__ __forceinline__ int warp_incl_scan(int v, int lane)
+{
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(FULL, v, o);
+        if (lane >= o) v += y;
+    }
+    return v;
+}
+
+template <int TPL>
+__global__ void __launch_bounds__(WALK_THREADS) k_walk(WalkParams p)
+{
+    extern __shared__ float4 walk_smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const int FL = p.flush, cap = FL + 32;
+    float4 *far = walk_smem + (size_t)warp * (2 * cap + cap / 4 + 1);
+    float4 *nearE = far + cap;
+    float *nearH = reinterpret_cast<float *>(nearE + cap);
+    int *stack = p.stack + (size_t)(blockIdx.x * WALK_WARPS + warp) * p.stack_cap;
+    const int ngroups = *p.ngroups;
+    const double theta = p.theta;
+
+    for (;;) {
+        int g = 0;
+        if (lane == 0) g = atomicAdd(p.group_counter, 1);
+        g = __shfl_sync(FULL, g, 0);
+        if (g >= ngroups) break;
+        const GGGroup grp = p.groups[g];
+
+        // ---- targets of the group
+        Targets<TPL> T;
+        double tx[TPL], ty[TPL], tz[TPL];
+        int tpi[TPL];
+        double bmin[3] = {INFINITY, INFINITY, INFINITY}, bmax[3] = {-INFINITY, -INFINITY, -INFINITY};
+        double aold_min = INFINITY;
+        float hmin = INFINITY, hmax = 0.f;
+#pragma unroll
+        for (int s = 0; s < TPL; s++) {
+            int k = s * 32 + lane;
+            bool v = k < grp.count;
+            T.valid[s] = v;
+            T.nint[s] = 0;
+            T.ax[s] = {0.f, 0.f}; T.ay[s] = {0.f, 0.f}; T.az[s] = {0.f, 0.f}; T.pot[s] = {0.f, 0.f};
+            tpi[s] = -1;
+            tx[s] = ty[s] = tz[s] = 0.0;
+            T.h[s] = 0.f;
+            if (v) {
+                int t = grp.first + k;
+                int pi = p.tlist ? p.tlist[t] : t;
+                tpi[s] = pi;
+                GGPart q = load_part(p.parts + pi);
+                tx[s] = q.x; ty[s] = q.y; tz[s] = q.z;
+                T.h[s] = q.h;
+                double oa = p.oldacc_in ? p.oldacc_in[p.perm[pi]] : 0.0;
+                aold_min = fmin(aold_min, p.tol * oa);
+                hmin = fminf(hmin, q.h);
+                hmax = fmaxf(hmax, q.h);
+                bmin[0] = fmin(bmin[0], q.x); bmax[0] = fmax(bmax[0], q.x);
+                bmin[1] = fmin(bmin[1], q.y); bmax[1] = fmax(bmax[1], q.y);
+                bmin[2] = fmin(bmin[2], q.z); bmax[2] = fmax(bmax[2], q.z);
+            }
+        }
+        double cg[3], hw[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            bmin[q] = warp_min_d(bmin[q]);
+            bmax[q] = warp_max_d(bmax[q]);
+            cg[q] = 0.5 * (bmin[q] + bmax[q]);
+            hw[q] = fmax(0.5 * (bmax[q] - bmin[q]), fmax(bmax[q] - cg[q], cg[q] - bmin[q]));
+        }
+        aold_min = warp_min_d(aold_min);
+        hmin = (float)warp_min_d((double)hmin);
+        hmax = (float)warp_max_d((double)hmax);
+#pragma unroll
+        for (int s = 0; s < TPL; s++) {
+            T.x[s] = (float)(tx[s] - cg[0]);
+            T.y[s] = (float)(ty[s] - cg[1]);
+            T.z[s] = (float)(tz[s] - cg[2]);
+        }
+        const double hmaxd = (double)hmax, hmind = (double)hmin;
+
+        // ---- traversal
+        int sp = 1, nf = 0, nn = 0;
+        bool overflow = false;
+        if (lane == 0) stack[0] = grp.root;
+        __syncwarp();
+        while (sp > 0) {
+            const int k = min(sp, 32);
+            const int base = sp - k;
+            int node = -1;
+            if (lane < k) node = stack[base + lane];
+            __syncwarp();
+            sp = base;
+
+            int act = 0, na = 0, nb = 0;
+            bool isfar = false;
+            float4 ent = make_float4(0.f, 0.f, 0.f, 0.f);
+            float hp = 0.f;
+            if (node >= 0) {
+                const GGNode nd = load_node(p.nodes + node);
+                na = nd.a;
+                nb = nd.b;
+                if (nd.mass > 0.f) {
+                    if (nb == -1) {
+                        act = 3;
+                    } else {
+                        double dx = nd.cx - cg[0], dy = nd.cy - cg[1], dz = nd.cz - cg[2];
+                        double ex = fmax(fabs(dx) - hw[0], 0.0), ey = fmax(fabs(dy) - hw[1], 0.0),
+                               ez = fmax(fabs(dz) - hw[2], 0.0);
+                        double r2 = ex * ex + ey * ey + ez * ez;
+                        double ms = (double)nd.maxsoft, L = (double)nd.len;
+                        bool open = (hmind < ms) && (r2 < ms * ms);
+                        if (!open) {
+                            if (theta > 0.0) {
+                                open = L * L > r2 * theta * theta;
+                            } else {
+                                double a1 = hmaxd + 0.6 * L, a2 = ms + 0.6 * L;
+                                open = (r2 < a1 * a1) || (r2 < a2 * a2) || ((double)nd.mass * L * L > r2 * r2 * aold_min);
+                                if (!open) {
+                                    double gx = fabs(dx + (double)nd.gx), gy = fabs(dy + (double)nd.gy),
+                                           gz = fabs(dz + (double)nd.gz);
+                                    open = (gx < 0.6 * L + hw[0]) && (gy < 0.6 * L + hw[1]) && (gz < 0.6 * L + hw[2]);
+                                }
+                            }
+                        }
+                        if (open) {
+                            act = (nb > 0) ? 2 : 3;
+                        } else {
+                            act = 1;
+                            ent = make_float4((float)dx, (float)dy, (float)dz, nd.mass);
+                            hp = nd.maxsoft;
+                            double hh = fmax(hmaxd, ms);
+                            isfar = (r2 >= hh * hh) && (r2 > 0.0);
+                        }
+                    }
+                }
+            }
+            // used nodes -> lists
+            {
+                unsigned mf = __ballot_sync(FULL, act == 1 && isfar);
+                unsigned mn = __ballot_sync(FULL, act == 1 && !isfar);
+                if (act == 1) {
+                    if (isfar) far[nf + __popc(mf & lt_mask)] = ent;
+                    else {
+                        int pos = nn + __popc(mn & lt_mask);
+                        nearE[pos] = ent;
+                        nearH[pos] = hp;
+                    }
+                }
+                nf += __popc(mf);
+                nn += __popc(mn);
+                if (nf >= FL) { flush_far<TPL>(far, nf, T); nf = 0; }
+                if (nn >= FL) { flush_near<TPL>(nearE, nearH, nn, T); nn = 0; }
+            }
+            // opened internal nodes -> children on the stack
+            {
+                int nch = (act == 2) ? nb : 0;
+                int incl = warp_incl_scan(nch, lane);
+                int total = __shfl_sync(FULL, incl, 31);
+                if (sp + total > p.stack_cap) {
+                    overflow = true;
+                    break;
+                }
+                int o = sp + incl - nch;
+                for (int c = 0; c < nch; c++) stack[o + c] = na + c;
+                sp += total;
+                __syncwarp();
+            }
+            // opened leaves -> particles, 32 at a time
+            {
+                int cnt = (act == 3) ? -nb : 0;
+                int incl = warp_incl_scan(cnt, lane);
+                int P = __shfl_sync(FULL, incl, 31);
+                int excl = incl - cnt;
+                for (int pb = 0; pb < P; pb += 32) {
+                    int q = pb + lane;
+                    int src = 0;
+#pragma unroll
+                    for (int step = 16; step > 0; step >>= 1) {
+                        int v = __shfl_sync(FULL, incl, src + step - 1);
+                        if (v <= q) src += step;
+                    }
+                    src = min(src, 31);
+                    int a_src = __shfl_sync(FULL, na, src);
+                    int e_src = __shfl_sync(FULL, excl, src);
+                    bool use = false, pfar = false;
+                    float4 pe = make_float4(0.f, 0.f, 0.f, 0.f);
+                    float ph = 0.f;
+                    if (q < P) {
+                        int pi = a_src + (q - e_src);
+                        GGPart pp = load_part(p.parts + pi);
+                        if (pp.m > 0.f) {
+                            double dx = pp.x - cg[0], dy = pp.y - cg[1], dz = pp.z - cg[2];
+                            double ex = fmax(fabs(dx) - hw[0], 0.0), ey = fmax(fabs(dy) - hw[1], 0.0),
+                                   ez = fmax(fabs(dz) - hw[2], 0.0);
+                            double r2 = ex * ex + ey * ey + ez * ez;
+                            double hh = fmax(hmaxd, (double)pp.h);
+                            pe = make_float4((float)dx, (float)dy, (float)dz, pp.m);
+                            ph = pp.h;
+                            use = true;
+                            pfar = (r2 >= hh * hh) && (r2 > 0.0);
+                        }
+                    }
+                    unsigned mf = __ballot_sync(FULL, use && pfar);
+                    unsigned mn = __ballot_sync(FULL, use && !pfar);
+                    if (use) {
+                        if (pfar) far[nf + __popc(mf & lt_mask)] = pe;
+                        else {
+                            int pos = nn + __popc(mn & lt_mask);
+                            nearE[pos] = pe;
+                            nearH[pos] = ph;
+                        }
+                    }
+                    nf += __popc(mf);
+                    nn += __popc(mn);
+                    if (nf >= FL) { flush_far<TPL>(far, nf, T); nf = 0; }
+                    if (nn >= FL) { flush_near<TPL>(nearE, nearH, nn, T); nn = 0; }
+                }
+            }
+        }
+        if (overflow) {
+            if (lane == 0) atomicOr(p.err, GG_EBIT_STACK_OVERFLOW);
+            continue;
+        }
+        if (nf > 0) flush_far<TPL>(far, nf, T);
+        if (nn > 0) flush_near<TPL>(nearE, nearH, nn, T);
+
+        // ---- results
+        int mycount = 0;
+#pragma unroll
+        for (int s = 0; s < TPL; s++) {
+            if (!T.valid[s]) continue;
+            int t = grp.first + s * 32 + lane;
+            int pi = tpi[s];
+            unsigned li = p.perm[pi];
+            int o = p.tout ? p.tout[t] : (int)li;
+            double ax = T.ax[s].value(), ay = T.ay[s].value(), az = T.az[s].value();
+            p.acc[3 * (size_t)o] = ax;
+            p.acc[3 * (size_t)o + 1] = ay;
+            p.acc[3 * (size_t)o + 2] = az;
+            if (p.pot) p.pot[o] = T.pot[s].value();
+            if (p.ninter) p.ninter[o] = T.nint[s];
+            if (p.oldacc_out) p.oldacc_out[li] = sqrt(ax * ax + ay * ay + az * az);
+            mycount += T.nint[s];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mycount += __shfl_xor_sync(FULL, mycount, o);
+        if (lane == 0) atomicAdd(p.interactions, (unsigned long long)mycount);
+    }
+}
+
+void gg_launch_walk(const WalkParams &p, int tpl, int blocks, cudaStream_t st)
+{
+    int smem = gg_walk_smem_bytes(p.flush, tpl);
+    if (tpl == 2) {
+        cudaFuncSetAttribute(k_walk<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        k_walk<2><<<blocks, WALK_THREADS, smem, st>>>(p);
+    } else {
+        cudaFuncSetAttribute(k_walk<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        k_walk<1><<<blocks, WALK_THREADS, smem, st>>>(p);
+    }
+    gg_note_launches(1);
+}

@@ -1,0 +1,300 @@
+"""Python binding (ctypes) of the B200 tree-gravity C ABI.
+
+The entry points mirror GIZMO's gravity interface (gravity/gravtree.c
+gravity_tree, gravity/forcetree.c force_treebuild / force_treeevaluate):
+accelerations and potentials are returned in GIZMO's pre-G units and the
+caller applies G (gravtree.c:495-501); OldAcc = |a|/G feeds the relative
+opening criterion of the next pass (gravtree.c:514-522).
+
+The CUDA library is required: every compute call raises GravityError when the
+shared library or a CUDA device is missing.  There is no CPU fallback.
+"""
+import ctypes
+import os
+import re
+import subprocess
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgizmo_gravity_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "gizmo_gravity_b200.h")
+
+GG_OK = 0
+ERRORS = {
+    -1: "GG_ERR_INVALID", -2: "GG_ERR_CUDA", -3: "GG_ERR_NOMEM", -4: "GG_ERR_OVERFLOW",
+    -5: "GG_ERR_TIMEOUT", -6: "GG_ERR_NOT_BUILT", -7: "GG_ERR_BAD_INPUT", -8: "GG_ERR_TOO_LARGE",
+}
+
+# one particle record on the device: {double x,y,z; float m; float h}
+PART_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("z", "<f8"), ("m", "<f4"), ("h", "<f4")])
+assert PART_DTYPE.itemsize == 32
+
+
+class GravityError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = status
+        msg = "%s (%d)" % (ERRORS.get(status, "unknown"), status)
+        if _lib is not None:
+            try:
+                msg += ": " + _lib.gg_strerror(status).decode()
+            except Exception:
+                pass
+        super().__init__((what + ": " if what else "") + msg)
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("leaf_size", ctypes.c_int32), ("group_size", ctypes.c_int32),
+                ("flush_threshold", ctypes.c_int32), ("walk_blocks_per_sm", ctypes.c_int32),
+                ("timing", ctypes.c_int32), ("reserved", ctypes.c_int32 * 2)]
+
+
+class Domain(ctypes.Structure):
+    _fields_ = [("center", ctypes.c_double * 3), ("corner", ctypes.c_double * 3), ("len", ctypes.c_double)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("interactions", ctypes.c_int64), ("n_nodes", ctypes.c_int64), ("n_targets", ctypes.c_int64),
+                ("n_groups", ctypes.c_int32), ("error_word", ctypes.c_int32), ("ms_keys", ctypes.c_double),
+                ("ms_sort", ctypes.c_double), ("ms_build", ctypes.c_double), ("ms_walk", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def build_library(force=False):
+    """Compile the CUDA library in-tree (nvcc, sm_100a)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-C", HERE, "-j8"], check=True, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
+    return LIB_PATH
+
+
+def header_functions():
+    """Function names declared in include/gizmo_gravity_b200.h."""
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(gg_[a-z0-9_]+)\s*\(", src)))
+
+
+def load_library():
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            build_library()
+        lib = ctypes.CDLL(LIB_PATH)
+        P = ctypes.c_void_p
+        i32, i64, dbl = ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+        sig = {
+            "gg_config_default": (None, [ctypes.POINTER(Config)]),
+            "gg_create": (i32, [ctypes.POINTER(Config), ctypes.POINTER(P)]),
+            "gg_destroy": (i32, [P]),
+            "gg_strerror": (ctypes.c_char_p, [i32]),
+            "gg_set_stream": (i32, [P, P]),
+            "gg_synchronize": (i32, [P]),
+            "gg_load_particles": (i32, [P, i32, P, P, i64, P, i64, P, i64]),
+            "gg_load_particles_device": (i32, [P, i32, P, P]),
+            "gg_build": (i32, [P, P]),
+            "gg_get_domains": (i32, [P, P]),
+            "gg_evaluate": (i32, [P, P, i64, P, dbl, dbl, P, P, P, ctypes.POINTER(Stats)]),
+            "gg_evaluate_device": (i32, [P, P, i64, P, dbl, dbl, P, P, P]),
+            "gg_last_stats": (i32, [P, ctypes.POINTER(Stats)]),
+            "gg_peano_hilbert_keys": (i32, [i64, P, ctypes.POINTER(Domain), P, P]),
+            "gg_radix_sort_pairs": (i32, [i64, P, P, i32, P]),
+            "gg_direct_sum_fp64": (i32, [i64, P, P, P, i64, P, P, P, P]),
+            "gg_fp32_peak_probe": (i32, [ctypes.POINTER(dbl), P]),
+            "gg_kernel_launches": (i64, []),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+        return lib
+
+
+def _check(status, what=""):
+    if status != GG_OK:
+        raise GravityError(status, what)
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return int(a.data_ptr())   # torch tensor
+
+
+def make_records(pos, mass, h):
+    """Pack (N,3) positions, masses and kernel radii into device record layout."""
+    pos = np.asarray(pos, dtype=np.float64)
+    rec = np.empty(pos.shape[0], dtype=PART_DTYPE)
+    rec["x"], rec["y"], rec["z"] = pos[:, 0], pos[:, 1], pos[:, 2]
+    rec["m"] = np.asarray(mass, dtype=np.float64)
+    rec["h"] = np.asarray(h, dtype=np.float64)
+    return rec
+
+
+def domain_to_dict(d):
+    return dict(center=list(d.center), corner=list(d.corner), len=d.len)
+
+
+class GravityTree:
+    """One library context: particles of one or more systems, their trees, walks."""
+
+    def __init__(self, leaf_size=8, group_size=64, flush=64, device=0, timing=False, blocks_per_sm=0):
+        lib = load_library()
+        cfg = Config()
+        lib.gg_config_default(ctypes.byref(cfg))
+        cfg.device, cfg.leaf_size, cfg.group_size, cfg.flush_threshold = device, leaf_size, group_size, flush
+        cfg.timing = 1 if timing else 0
+        cfg.walk_blocks_per_sm = blocks_per_sm
+        h = ctypes.c_void_p()
+        _check(lib.gg_create(ctypes.byref(cfg), ctypes.byref(h)), "gg_create")
+        self._lib, self._h = lib, h
+        self.n = 0
+        self.counts = None
+
+    def close(self):
+        if self._h:
+            self._lib.gg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_stream(self, stream_ptr):
+        _check(self._lib.gg_set_stream(self._h, stream_ptr), "gg_set_stream")
+
+    def synchronize(self):
+        _check(self._lib.gg_synchronize(self._h), "gg_synchronize")
+
+    def load(self, pos, mass, h, counts=None):
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        mass = np.ascontiguousarray(mass, dtype=np.float64)
+        h = np.ascontiguousarray(h, dtype=np.float64)
+        n = pos.shape[0]
+        counts = np.asarray([n] if counts is None else counts, dtype=np.int64)
+        _check(self._lib.gg_load_particles(self._h, len(counts), counts.ctypes.data, pos.ctypes.data, 24,
+                                           mass.ctypes.data, 8, h.ctypes.data, 8), "gg_load_particles")
+        self.n, self.counts = n, counts
+        self._keep = (pos, mass, h, counts)
+
+    def load_device(self, records, counts):
+        """records: device buffer (torch uint8/any tensor) holding N 32-byte records."""
+        counts = np.asarray(counts, dtype=np.int64)
+        _check(self._lib.gg_load_particles_device(self._h, len(counts), counts.ctypes.data, _ptr(records)),
+               "gg_load_particles_device")
+        self.n, self.counts = int(counts.sum()), counts
+
+    def build(self, domains=None):
+        arr = None
+        if domains is not None:
+            arr = (Domain * len(domains))()
+            for i, d in enumerate(domains):
+                arr[i].center[:] = list(d["center"])
+                arr[i].corner[:] = list(d["corner"])
+                arr[i].len = d["len"]
+        _check(self._lib.gg_build(self._h, arr), "gg_build")
+
+    def domains(self):
+        arr = (Domain * len(self.counts))()
+        _check(self._lib.gg_get_domains(self._h, arr), "gg_get_domains")
+        return [domain_to_dict(d) for d in arr]
+
+    def evaluate(self, active=None, old_acc=None, err_tol_force_acc=0.0025, err_tol_theta=0.0, want_ninter=False):
+        """Walk the trees for `active` particles (None = all).  Returns (acc, pot, ninter|None, stats)."""
+        act = None
+        if active is not None:
+            act = np.ascontiguousarray(active, dtype=np.int32)
+        nt = self.n if act is None else act.shape[0]
+        acc = np.empty((nt, 3), dtype=np.float64)
+        pot = np.empty(nt, dtype=np.float64)
+        nint = np.empty(nt, dtype=np.int64) if want_ninter else None
+        oa = None if old_acc is None else np.ascontiguousarray(old_acc, dtype=np.float64)
+        st = Stats()
+        _check(self._lib.gg_evaluate(self._h, None if act is None else act.ctypes.data, nt,
+                                     None if oa is None else oa.ctypes.data, err_tol_force_acc, err_tol_theta,
+                                     acc.ctypes.data, pot.ctypes.data, None if nint is None else nint.ctypes.data,
+                                     ctypes.byref(st)), "gg_evaluate")
+        return acc, pot, nint, st.as_dict()
+
+    def evaluate_device(self, d_acc, d_pot=None, d_active=None, n_active=0, d_old_acc=None, err_tol_force_acc=0.0025,
+                        err_tol_theta=0.0, d_ninter=None):
+        _check(self._lib.gg_evaluate_device(self._h, _ptr(d_active), n_active, _ptr(d_old_acc), err_tol_force_acc,
+                                            err_tol_theta, _ptr(d_acc), _ptr(d_pot), _ptr(d_ninter)),
+               "gg_evaluate_device")
+
+    def last_stats(self):
+        st = Stats()
+        _check(self._lib.gg_last_stats(self._h, ctypes.byref(st)), "gg_last_stats")
+        return st.as_dict()
+
+
+def gravity_tree(pos, mass, h, G=1.0, err_tol_force_acc=0.0025, err_tol_theta=0.7, active=None, tree=None,
+                 **cfg):
+    """GIZMO's start-up force evaluation (accel.c:47-50): a Barnes-Hut pass with
+    ErrTolTheta (begrun.c:2368) gives OldAcc, then the relative pass with
+    ErrTolForceAcc (begrun.c:2369).  Returns acc*G, pot*G, OldAcc, stats of the
+    relative pass (gravtree.c:495-522)."""
+    own = tree is None
+    t = tree or GravityTree(**cfg)
+    try:
+        t.load(pos, mass, h)
+        t.build()
+        a1, _, _, _ = t.evaluate(active=None, err_tol_theta=err_tol_theta)
+        old = np.linalg.norm(a1, axis=1)   # |a| in pre-G units == OldAcc (|a G| / G)
+        acc, pot, nint, st = t.evaluate(active=active, old_acc=old, err_tol_force_acc=err_tol_force_acc,
+                                        err_tol_theta=0.0)
+        acc_active_old = np.linalg.norm(acc, axis=1)
+        return acc * G, pot * G, acc_active_old, st
+    finally:
+        if own:
+            t.close()
+
+
+def peano_hilbert_keys(d_pos, n, domain, d_keys, stream=None):
+    lib = load_library()
+    d = Domain()
+    d.center[:] = list(domain["center"])
+    d.corner[:] = list(domain["corner"])
+    d.len = domain["len"]
+    _check(lib.gg_peano_hilbert_keys(n, _ptr(d_pos), ctypes.byref(d), _ptr(d_keys), stream), "gg_peano_hilbert_keys")
+
+
+def radix_sort_pairs(d_keys, d_vals, n, key_bits=64, stream=None):
+    lib = load_library()
+    _check(lib.gg_radix_sort_pairs(n, _ptr(d_keys), _ptr(d_vals), key_bits, stream), "gg_radix_sort_pairs")
+
+
+def direct_sum_fp64(d_pos, d_mass, d_h, n_src, d_targets, n_tgt, d_acc, d_pot, stream=None):
+    lib = load_library()
+    _check(lib.gg_direct_sum_fp64(n_src, _ptr(d_pos), _ptr(d_mass), _ptr(d_h), n_tgt, _ptr(d_targets), _ptr(d_acc),
+                                  _ptr(d_pot), stream), "gg_direct_sum_fp64")
+
+
+def fp32_peak_tflops(stream=None):
+    lib = load_library()
+    v = ctypes.c_double()
+    _check(lib.gg_fp32_peak_probe(ctypes.byref(v), stream), "gg_fp32_peak_probe")
+    return v.value
+
+
+def kernel_launches():
+    return int(load_library().gg_kernel_launches())

@@ -1,0 +1,152 @@
+/*
+ * gizmo_gravity_b200.h -- C ABI of the B200 tree-gravity library.
+ *
+ * The library replaces GIZMO's tree-gravity force evaluation: the Peano-Hilbert
+ * keys and sort (system/peano.c, domain.c), the oct-tree build with monopole
+ * moments (gravity/forcetree.c force_treebuild / force_update_node_recursive)
+ * and the tree walk (gravity/forcetree.c force_treeevaluate, driven by
+ * gravity_tree in gravity/gravtree.c).  GIZMO selects it with the compile
+ * flag GRAVITY_GPU_B200 inside gravity_tree(); kicks, timesteps and the
+ * active-particle list are unchanged.
+ *
+ * Conventions (all paths below are within the GIZMO source tree):
+ *   - accelerations and potentials come back in GIZMO's pre-G units: the walk
+ *     accumulates sum m*dx/r^3 and the caller multiplies by All.G
+ *     (gravity/gravtree.c:495, :501);
+ *   - softening is passed as the kernel radius h = 2.8 * Plummer epsilon,
+ *     i.e. ForceSoftening_KernelRadius() (proto.h:134-155, gravtree.c:774);
+ *   - err_tol_theta > 0 selects the Barnes-Hut pass, err_tol_theta == 0 the
+ *     relative criterion with err_tol_force_acc (forcetree.c:2104-2158);
+ *   - old_acc is |a|/G of the previous pass, P[i].OldAcc (gravtree.c:514-522).
+ *
+ * Several independent systems can be loaded at once ("systems", each with its
+ * own root cube and tree); a GIZMO rank uses one.  No function traps on the
+ * device: kernels record failures in an error word and the call returns a
+ * negative gg_status.  A context is not re-entrant; use one per host thread.
+ */
+#ifndef GIZMO_GRAVITY_B200_H
+#define GIZMO_GRAVITY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t gg_status;
+
+enum {
+    GG_OK = 0,
+    GG_ERR_INVALID = -1,      /* bad argument (null pointer, negative size, ...) */
+    GG_ERR_CUDA = -2,         /* CUDA runtime error or no usable device */
+    GG_ERR_NOMEM = -3,        /* device allocation failed */
+    GG_ERR_OVERFLOW = -4,     /* node pool or walk stack overflow */
+    GG_ERR_TIMEOUT = -5,      /* a bounded device-side wait gave up */
+    GG_ERR_NOT_BUILT = -6,    /* gg_evaluate before gg_build */
+    GG_ERR_BAD_INPUT = -7,    /* non-finite position, or positions outside the cube */
+    GG_ERR_TOO_LARGE = -8     /* size beyond a fixed limit of the call */
+};
+
+typedef struct gg_config {
+    int32_t device;           /* CUDA device ordinal */
+    int32_t leaf_size;        /* max particles per leaf bucket, 1..32 (default 8) */
+    int32_t group_size;       /* targets per walk group, 1..64 (default 64) */
+    int32_t flush_threshold;  /* interaction-list entries per flush, 32..128 (default 64) */
+    int32_t walk_blocks_per_sm; /* persistent walk blocks per SM, 0 = default */
+    int32_t timing;           /* 1: record per-stage device times into gg_stats */
+    int32_t reserved[2];
+} gg_config;
+
+/* root cube of one system: domain_findExtent (domain.c:2518-2570) */
+typedef struct gg_domain {
+    double center[3];
+    double corner[3];
+    double len;
+} gg_domain;
+
+typedef struct gg_stats {
+    int64_t interactions;   /* sum over targets of used nodes/particles with r2>0 && m>0
+                               (the reference's Costtotal, gravtree.c:700) */
+    int64_t n_nodes;        /* tree nodes over all systems */
+    int64_t n_targets;      /* targets walked */
+    int32_t n_groups;       /* walk groups */
+    int32_t error_word;     /* device error bits of the last call */
+    double ms_keys;         /* extent + keys (device time, when timing is on) */
+    double ms_sort;
+    double ms_build;        /* permute + tree + moments */
+    double ms_walk;
+} gg_stats;
+
+typedef struct gg_ctx gg_ctx;
+
+/* ---- context ------------------------------------------------------------ */
+void gg_config_default(gg_config *cfg);
+gg_status gg_create(const gg_config *cfg, gg_ctx **out);
+gg_status gg_destroy(gg_ctx *ctx);
+const char *gg_strerror(gg_status s);
+/* run this context's work on an existing cudaStream_t (NULL: the ctx's own) */
+gg_status gg_set_stream(gg_ctx *ctx, void *cuda_stream);
+gg_status gg_synchronize(gg_ctx *ctx);
+
+/* ---- particles -----------------------------------------------------------
+ * Replaces the particle gather of force_treebuild (forcetree.c:109) and the
+ * P[] loads of force_treeevaluate (forcetree.c:1850-1968).  Host arrays may be
+ * strided: GIZMO passes &P[0].Pos[0], sizeof(struct particle_data), and so on.
+ * counts[n_systems] gives each system's particle count; particles of system s
+ * follow those of system s-1.  Masses are stored in FP32 on the device. */
+gg_status gg_load_particles(gg_ctx *ctx, int32_t n_systems, const int64_t *counts, const double *pos,
+                            int64_t pos_stride_bytes, const double *mass, int64_t mass_stride_bytes,
+                            const double *soft_h, int64_t soft_stride_bytes);
+/* device-resident records {double x,y,z; float mass; float h} (32 bytes each) */
+gg_status gg_load_particles_device(gg_ctx *ctx, int32_t n_systems, const int64_t *counts, const void *d_records);
+
+/* ---- build -------------------------------------------------------------
+ * domain_findExtent (domain.c:2518) + keys (domain.c:2236-2262, peano.c:303)
+ * + sort (peano.c:28-92) + force_treebuild (forcetree.c:109-342) +
+ * force_update_node_recursive (forcetree.c:434-942).  domains == NULL: the
+ * root cube of each system is found on the device like domain_findExtent. */
+gg_status gg_build(gg_ctx *ctx, const gg_domain *domains);
+gg_status gg_get_domains(gg_ctx *ctx, gg_domain *out);
+
+/* ---- walk --------------------------------------------------------------
+ * The force_treeevaluate loop of gravity_tree (gravtree.c:138-457).
+ * active: indices of the particles to evaluate (NULL = all, in load order);
+ * old_acc: per particle |a|/G in load order (NULL = the values the previous
+ * evaluation of this context left on the device, or 0 before the first).
+ * Outputs (per active particle, in the order of `active`): acc_out n*3 and
+ * pot_out n (pre-G), ninter_out n (nullable each).  Blocking. */
+gg_status gg_evaluate(gg_ctx *ctx, const int32_t *active, int64_t n_active, const double *old_acc,
+                      double err_tol_force_acc, double err_tol_theta, double *acc_out, double *pot_out,
+                      int64_t *ninter_out, gg_stats *stats);
+/* Same on device pointers, asynchronous on the context's stream. */
+gg_status gg_evaluate_device(gg_ctx *ctx, const int32_t *d_active, int64_t n_active, const double *d_old_acc,
+                             double err_tol_force_acc, double err_tol_theta, double *d_acc_out,
+                             double *d_pot_out, int32_t *d_ninter_out);
+/* interaction count and error word of the last evaluation (synchronises) */
+gg_status gg_last_stats(gg_ctx *ctx, gg_stats *stats);
+
+/* ---- kernel-level entry points (device pointers, cudaStream_t or NULL) ---- */
+/* domain_double_to_int (domain.c:2504-2513) + peano_hilbert_key (peano.c:303-319)
+ * at 21 bits per dimension: equals the reference's 42-bit key shifted right by 63 */
+gg_status gg_peano_hilbert_keys(int64_t n, const double *d_pos, const gg_domain *dom, uint64_t *d_keys,
+                                void *stream);
+/* stable LSD radix sort of (key, value) pairs, replacing mysort_peano
+ * (peano.c:414-462); key_bits <= 64; scratch is allocated by the call */
+gg_status gg_radix_sort_pairs(int64_t n, uint64_t *d_keys, uint32_t *d_vals, int32_t key_bits, void *stream);
+/* FP64 direct summation over all sources with the walk's pair rule (the
+ * reference declares force_treeevaluate_direct, gravity/forcetree.h:76, but
+ * ships no definition); used to measure force errors at full size */
+gg_status gg_direct_sum_fp64(int64_t n_src, const double *d_pos, const double *d_mass, const double *d_h,
+                             int64_t n_tgt, const int32_t *d_targets, double *d_acc, double *d_pot, void *stream);
+
+/* measured FP32 FMA throughput of the device in TFLOP/s (2 flops per FMA):
+ * the CUDA-core roofline the walk is reported against */
+gg_status gg_fp32_peak_probe(double *tflops, void *stream);
+/* kernels this library has launched in this process (all contexts) */
+int64_t gg_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

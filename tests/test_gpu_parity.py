@@ -1,0 +1,236 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle."""
+import numpy as np
+import pytest
+
+import ggb200
+import ics
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def torch_cuda():
+    import torch
+    return torch
+
+
+def test_keys_bitwise_equal_oracle():
+    torch = torch_cuda()
+    rng = np.random.default_rng(21)
+    pos = np.concatenate([rng.normal(size=(50000, 3)), rng.uniform(-3, 3, size=(50000, 3)),
+                          ics.plummer(20000, seed=5)["pos"]])
+    d = oracle.find_extent(pos)
+    hi, lo = oracle.ph_keys(pos, d, bits=21)
+    assert np.all(hi == 0)
+    dpos = torch.from_numpy(pos).cuda()
+    dkeys = torch.empty(pos.shape[0], dtype=torch.int64, device="cuda")
+    ggb200.peano_hilbert_keys(dpos, pos.shape[0], d, dkeys)
+    torch.cuda.synchronize()
+    got = dkeys.cpu().numpy().view(np.uint64)
+    assert np.array_equal(got, lo)
+
+
+@pytest.mark.parametrize("n", [2, 3, 4095, 4096, 4097, 100003, 1 << 20])
+def test_radix_sort_is_stable_and_exact(n):
+    torch = torch_cuda()
+    rng = np.random.default_rng(n)
+    keys = rng.integers(0, 1 << 63, size=n, dtype=np.uint64)
+    keys[: n // 3] = keys[n // 3: 2 * (n // 3)] if n >= 3 else keys[: n // 3]   # duplicates
+    keys[::7] &= np.uint64(0xFFFF)   # many small keys
+    vals = np.arange(n, dtype=np.uint32)
+    order = np.argsort(keys, kind="stable")
+    dk = torch.from_numpy(keys.view(np.int64).copy()).cuda()
+    dv = torch.from_numpy(vals.view(np.int32).copy()).cuda()
+    ggb200.radix_sort_pairs(dk, dv, n, 64)
+    torch.cuda.synchronize()
+    assert np.array_equal(dk.cpu().numpy().view(np.uint64), keys[order])
+    assert np.array_equal(dv.cpu().numpy().view(np.uint32), vals[order])
+
+
+def test_extent_bitwise_equal_oracle():
+    ic = ics.plummer(30000, seed=31)
+    with ggb200.GravityTree() as t:
+        t.load(ic["pos"], ic["mass"], ic["h"])
+        t.build()
+        d = t.domains()[0]
+    ref = oracle.find_extent(ic["pos"])
+    assert d["len"] == ref["len"]
+    assert d["center"] == ref["center"] and d["corner"] == ref["corner"]
+
+
+def _exact_tree():
+    # one-particle leaves and one-target groups: the reference's node set and tests
+    return ggb200.GravityTree(leaf_size=1, group_size=1)
+
+
+@pytest.mark.parametrize("theta", [0.7, 0.0])
+def test_exact_mode_matches_oracle_interactions_and_forces(theta):
+    ic = ics.plummer(4096, seed=41)
+    pos, mass, h = ic["pos"], ic["mass"], ic["h"]
+    acc_bh, _, _, _ = oracle.tree_gravity(pos, mass, h, None, 0.0025, 0.7)
+    old = np.linalg.norm(acc_bh, axis=1)
+    acc_o, pot_o, nint_o, tot_o = oracle.tree_gravity(pos, mass, h, old, 0.0025, theta)
+    with _exact_tree() as t:
+        t.load(pos, mass, h)
+        t.build()
+        acc, pot, nint, st = t.evaluate(old_acc=old, err_tol_force_acc=0.0025, err_tol_theta=theta, want_ninter=True)
+    # interaction sets: the same tests in FP64 on centres of mass summed in another order
+    mism = np.count_nonzero(nint != nint_o)
+    assert mism <= 2, (mism, np.abs(nint - nint_o).max())
+    assert abs(st["interactions"] - tot_o) <= 8
+    ok = nint == nint_o
+    rel = np.linalg.norm(acc - acc_o, axis=1) / np.linalg.norm(acc_o, axis=1)
+    assert np.percentile(rel[ok], 99) < 2e-5 and rel[ok].max() < 2e-4   # FP32 arithmetic
+    assert np.allclose(pot[ok], pot_o[ok], rtol=2e-5)
+
+
+def _two_pass(t, ic, tol=0.0025, active=None):
+    t.load(ic["pos"], ic["mass"], ic["h"])
+    t.build()
+    a1, _, _, _ = t.evaluate(err_tol_theta=0.7)
+    return t.evaluate(active=active, old_acc=np.linalg.norm(a1, axis=1), err_tol_force_acc=tol, want_ninter=True)
+
+
+@pytest.mark.parametrize("model,n", [("plummer", 16384), ("galaxy", 20000), ("clustered", 20000)])
+def test_default_walk_error_within_reference_bound(model, n):
+    if model == "plummer":
+        ic = ics.plummer(n, seed=51)
+    elif model == "galaxy":
+        ic = ics.galaxy(n_halo=int(n * 0.715), n_disk=n - int(n * 0.715), seed=52)
+    else:
+        ic = ics.clustered(n, seed=53, n_clumps=20)
+    pos, mass, h = ic["pos"], ic["mass"], ic["h"]
+    acc_d, pot_d = oracle.direct_sum(pos, mass, h)
+    acc_o, pot_o, _, tot_o, _ = oracle.tree_gravity_two_pass(pos, mass, h, 0.0025)
+    with ggb200.GravityTree() as t:
+        acc, pot, nint, st = _two_pass(t, ic)
+    p50_o, p99_o, _ = ics.error_stats(acc_o, acc_d)
+    p50, p99, _ = ics.error_stats(acc, acc_d)
+    assert p50 <= 1.1 * p50_o and p99 <= 1.1 * p99_o, (p50, p99, p50_o, p99_o)
+    # potential energy W = 1/2 sum m phi against the FP64 direct sum
+    W, Wd, Wo = 0.5 * np.sum(mass * pot), 0.5 * np.sum(mass * pot_d), 0.5 * np.sum(mass * pot_o)
+    assert abs(W - Wd) <= max(abs(Wo - Wd), 1e-5 * abs(Wd))
+    assert st["error_word"] == 0
+
+
+def test_active_subset_exact_mode_is_independent_of_the_rest():
+    ic = ics.plummer(8192, seed=61)
+    act = ics.random_active(8192, 0.1, seed=62)
+    with _exact_tree() as t:
+        t.load(ic["pos"], ic["mass"], ic["h"])
+        t.build()
+        a1, _, _, _ = t.evaluate(err_tol_theta=0.7)
+        old = np.linalg.norm(a1, axis=1)
+        full, pf, nf, _ = t.evaluate(old_acc=old, want_ninter=True)
+        sub, ps, ns, st = t.evaluate(active=act, old_acc=old, want_ninter=True)
+    assert np.array_equal(sub, full[act]) and np.array_equal(ps, pf[act]) and np.array_equal(ns, nf[act])
+    assert st["n_targets"] == act.size
+
+
+def test_active_subset_default_mode_error():
+    ic = ics.plummer(16384, seed=63)
+    act = ics.random_active(16384, 0.1, seed=64)
+    acc_d, _ = oracle.direct_sum(ic["pos"], ic["mass"], ic["h"], targets=act)
+    a, _, _, _, _ = oracle.tree_gravity_two_pass(ic["pos"], ic["mass"], ic["h"], 0.0025, targets=act)
+    with ggb200.GravityTree() as t:
+        acc, _, _, _ = _two_pass(t, ic, active=act)
+    assert ics.error_stats(acc, acc_d)[1] <= 1.1 * ics.error_stats(a, acc_d)[1]
+
+
+def test_systems_alone_equal_systems_together():
+    a = ics.plummer(5000, seed=71)
+    b = ics.plummer(3000, seed=72)
+    b["pos"] = b["pos"] * 0.5 + 3.0
+    res = []
+    for ic in (a, b):
+        with ggb200.GravityTree() as t:
+            res.append(_two_pass(t, ic))
+    with ggb200.GravityTree() as t:
+        pos = np.concatenate([a["pos"], b["pos"]])
+        mass = np.concatenate([a["mass"], b["mass"]])
+        h = np.concatenate([a["h"], b["h"]])
+        t.load(pos, mass, h, counts=[5000, 3000])
+        t.build()
+        a1, _, _, _ = t.evaluate(err_tol_theta=0.7)
+        acc, pot, nint, _ = t.evaluate(old_acc=np.linalg.norm(a1, axis=1), want_ninter=True)
+    assert np.array_equal(acc[:5000], res[0][0]) and np.array_equal(acc[5000:], res[1][0])
+    assert np.array_equal(pot[:5000], res[0][1]) and np.array_equal(nint[5000:], res[1][2])
+
+
+def test_edge_cases_tiny_and_degenerate():
+    with ggb200.GravityTree() as t:
+        # one particle: no force
+        t.load(np.zeros((1, 3)), np.ones(1), np.full(1, 0.1))
+        t.build()
+        acc, pot, nint, _ = t.evaluate(err_tol_theta=0.7, want_ninter=True)
+        assert np.all(acc == 0) and nint[0] == 0
+        # two particles far apart: Newtonian pair force
+        pos = np.array([[0.0, 0, 0], [2.0, 0, 0]])
+        t.load(pos, np.array([1.0, 3.0]), np.full(2, 0.1))
+        t.build()
+        acc, pot, nint, _ = t.evaluate(err_tol_theta=0.7, want_ninter=True)
+        assert acc[0] == pytest.approx([3.0 / 4, 0, 0], rel=1e-6)
+        assert acc[1] == pytest.approx([-1.0 / 4, 0, 0], rel=1e-6)
+        assert pot[0] == pytest.approx(-1.5, rel=1e-6)
+        # many coincident particles (leaf chunks at full key depth) and zero masses
+        rng = np.random.default_rng(81)
+        pos = np.concatenate([np.zeros((300, 3)), rng.normal(size=(700, 3))])
+        mass = np.full(1000, 1e-3)
+        mass[::10] = 0.0
+        h = np.full(1000, 0.05)
+        acc_d, _ = oracle.direct_sum(pos, mass, h)
+        t.load(pos, mass, h)
+        t.build()
+        a1, _, _, st = t.evaluate(err_tol_theta=0.0, old_acc=np.zeros(1000))   # opens everything: direct sum
+        assert st["error_word"] == 0
+        assert np.allclose(a1, acc_d, rtol=1e-4, atol=1e-6 * np.abs(acc_d).max())
+
+
+def test_non_finite_position_is_rejected():
+    pos = np.random.default_rng(82).normal(size=(100, 3))
+    pos[17, 1] = np.nan
+    with ggb200.GravityTree() as t:
+        t.load(pos, np.ones(100), np.full(100, 0.1))
+        t.build()
+        with pytest.raises(ggb200.GravityError) as ei:
+            t.evaluate(err_tol_theta=0.7)
+        assert ei.value.status == -7
+
+
+def test_direct_sum_kernel_matches_oracle():
+    torch = torch_cuda()
+    ic = ics.plummer(6000, seed=91)
+    tg = np.arange(0, 6000, 7, dtype=np.int32)
+    acc_o, pot_o = oracle.direct_sum(ic["pos"], ic["mass"], ic["h"], targets=tg)
+    dp = torch.from_numpy(ic["pos"]).cuda()
+    dm = torch.from_numpy(ic["mass"]).cuda()
+    dh = torch.from_numpy(ic["h"]).cuda()
+    dt = torch.from_numpy(tg).cuda()
+    da = torch.empty((tg.size, 3), dtype=torch.float64, device="cuda")
+    dpo = torch.empty(tg.size, dtype=torch.float64, device="cuda")
+    ggb200.direct_sum_fp64(dp, dm, dh, 6000, dt, tg.size, da, dpo)
+    torch.cuda.synchronize()
+    assert np.allclose(da.cpu().numpy(), acc_o, rtol=1e-11, atol=1e-13)
+    assert np.allclose(dpo.cpu().numpy(), pot_o, rtol=1e-11)
+
+
+def test_full_size_galaxy_properties():
+    """At the benchmark size: error against the GPU FP64 direct sum on a subsample,
+    momentum balance, and run-to-run bitwise determinism."""
+    torch = torch_cuda()
+    ic = ics.galaxy()
+    n = ic["pos"].shape[0]
+    with ggb200.GravityTree() as t:
+        acc, pot, nint, st = _two_pass(t, ic)
+        acc2, _, _, _ = t.evaluate(old_acc=None)   # re-walk with device-resident OldAcc
+    assert st["error_word"] == 0
+    tg = np.sort(np.random.default_rng(5).choice(n, 4096, replace=False)).astype(np.int32)
+    dp, dm, dh = (torch.from_numpy(ic[k]).cuda() for k in ("pos", "mass", "h"))
+    da = torch.empty((tg.size, 3), dtype=torch.float64, device="cuda")
+    ggb200.direct_sum_fp64(dp, dm, dh, n, torch.from_numpy(tg).cuda(), tg.size, da, None)
+    torch.cuda.synchronize()
+    p50, p99, _ = ics.error_stats(acc[tg], da.cpu().numpy())
+    assert p99 < 5e-3, (p50, p99)
+    ptot = (ic["mass"][:, None] * acc).sum(0)
+    assert np.linalg.norm(ptot) < 1e-3 * (ic["mass"][:, None] * np.abs(acc)).sum()
+    assert st["interactions"] == nint.sum()
