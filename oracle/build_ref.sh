@@ -1,0 +1,59 @@
+#!/bin/bash
+# Builds the reference code itself as a CPU oracle / CPU baseline:
+# GIZMO's own sources, read where they lie in the reference tree, compiled
+# against project-written single-rank MPI and minimal GSL stand-ins (shim/)
+# and linked with ref_main.c instead of main.c.  Output: oracle/_ref/gizmo_ref.
+# Nothing from the reference tree is copied into the repository: the compile
+# reads a symlink mirror under a temporary directory, needed only so that the
+# reference's relative include of ../GIZMO_config.h resolves to shim/GIZMO_config.h.
+# TEST INFRASTRUCTURE ONLY.
+set -euo pipefail
+HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REF="${GIZMO_REF:-/root/reference}"
+OUT="$HERE/_ref"
+CC=/usr/bin/gcc
+# x86-64-v3 (AVX2/FMA): the binary runs on the GPU hosts as well as here
+CFLAGS="-O3 -march=x86-64-v3 -fopenmp -std=gnu99 -w"
+if [ ! -d "$REF" ]; then echo "reference tree not found: $REF" >&2; exit 1; fi
+if [ -x "$OUT/gizmo_ref" ] && [ "$OUT/gizmo_ref" -nt "$HERE/ref_main.c" ] && [ "$OUT/gizmo_ref" -nt "$0" ]; then
+  echo "oracle/_ref/gizmo_ref is up to date"; exit 0
+fi
+MIRROR="$(mktemp -d /tmp/gg_ref_src.XXXXXX)"
+trap 'rm -rf "$MIRROR"' EXIT
+cp -rs "$REF/." "$MIRROR/"
+cp "$HERE/shim/GIZMO_config.h" "$MIRROR/GIZMO_config.h"
+mkdir -p "$OUT/obj"
+cd "$MIRROR"
+# the object list of the reference Makefile (CORE..MISC groups) without main.o
+# and the generated compile_time_info.o
+FILES="accel.c timestep.c init.c restart.c io.c predict.c global.c begrun.c run.c allvars.c read_ic.c domain.c
+driftfac.c kicks.c ngb.c merge_split.c system/system.c system/allocate.c system/mymalloc.c system/parallel_sort.c
+system/peano.c system/parallel_sort_special.c system/mpi_util.c system/pinning.c gravity/forcetree.c
+gravity/forcetree_update.c gravity/gravtree.c gravity/cosmology.c gravity/potential.c gravity/pm_periodic.c
+gravity/pm_nonperiodic.c gravity/longrange.c gravity/ags_hsml.c gravity/binary.c hydro/hydro_toplevel.c
+hydro/density.c hydro/gradients.c turb/dynamic_diffusion.c turb/dynamic_diffusion_velocities.c turb/turb_driving.c
+turb/turb_powerspectra.c cooling/cooling.c cooling/grackle.c eos/eos.c eos/hydrogen_molecule.c
+eos/cosmic_ray_fluid/cosmic_ray_alfven.c eos/cosmic_ray_fluid/cosmic_ray_utilities.c solids/elastic_physics.c
+solids/grain_physics.c solids/ism_dust_chemistry.c nuclear/nuclear_network_solver.c nuclear/nuclear_network.c
+galaxy_sf/sfr_eff.c galaxy_sf/stellar_evolution.c galaxy_sf/mechanical_fb.c galaxy_sf/thermal_fb.c
+galaxy_sf/radfb_local.c galaxy_sf/dm_dispersion_hsml.c galaxy_sf/blackholes/blackhole.c
+galaxy_sf/blackholes/blackhole_util.c galaxy_sf/blackholes/blackhole_environment.c galaxy_sf/blackholes/blackhole_feed.c
+galaxy_sf/blackholes/blackhole_swallow_and_kick.c radiation/rt_utilities.c radiation/rt_CGmethod.c
+radiation/rt_source_injection.c radiation/rt_chem.c radiation/rt_cooling.c structure/fof.c structure/subfind/subfind.c
+structure/subfind/subfind_vars.c structure/subfind/subfind_collective.c structure/subfind/subfind_serial.c
+structure/subfind/subfind_so.c structure/subfind/subfind_cont.c structure/subfind/subfind_distribute.c
+structure/subfind/subfind_findlinkngb.c structure/subfind/subfind_nearesttwo.c structure/subfind/subfind_loctree.c
+structure/subfind/subfind_potential.c structure/subfind/subfind_density.c structure/twopoint.c structure/lineofsight.c
+sidm/cbe_integrator.c sidm/dm_fuzzy.c sidm/sidm_core.c"
+OBJS=""
+for f in $FILES; do
+  o="$OUT/obj/$(echo "$f" | tr / _ | sed 's/\.c$/.o/')"
+  OBJS="$OBJS $o"
+  echo "$CC $CFLAGS -I$HERE/shim -I$MIRROR -c $f -o $o"
+done > "$MIRROR/cmds.sh"
+xargs -P "$(nproc)" -I{} bash -c '{}' < "$MIRROR/cmds.sh"
+$CC $CFLAGS -I"$HERE/shim" -I"$MIRROR" -c "$HERE/ref_main.c" -o "$OUT/obj/ref_main.o"
+$CC $CFLAGS -I"$HERE/shim" -c "$HERE/shim/mpi_single.c" -o "$OUT/obj/mpi_single.o"
+$CC $CFLAGS -I"$HERE/shim" -c "$HERE/shim/gsl_shim.c" -o "$OUT/obj/gsl_shim.o"
+$CC $CFLAGS -o "$OUT/gizmo_ref" $OBJS "$OUT/obj/ref_main.o" "$OUT/obj/mpi_single.o" "$OUT/obj/gsl_shim.o" -lm
+echo "built $OUT/gizmo_ref"

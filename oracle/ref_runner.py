@@ -1,0 +1,232 @@
+"""Run the reference code itself (oracle/_ref/gizmo_ref, built by build_ref.sh).
+
+TEST INFRASTRUCTURE ONLY: used by tests/golden/make_golden.py to produce
+golden vectors, and by bench.py's reference arm / CPU baseline to time the
+reference's own OpenMP tree gravity on the host cores.
+
+Initial conditions go to the reference in its unformatted format-1 binary
+(read_ic.c:721-730): a 256-byte header block, then POS, VEL, ID and MASS
+blocks, each framed by Fortran record markers, positions and masses in FP64
+(INPUT_IN_DOUBLEPRECISION).  Particle types carry the per-type softenings
+(SofteningHalo = type 1, SofteningDisk = type 2).
+"""
+import os
+import struct
+import subprocess
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BIN = os.path.join(HERE, "_ref", "gizmo_ref")
+KERNEL_FAC = 2.8
+
+
+def available():
+    if not os.path.exists(BIN):
+        return False
+    try:
+        r = subprocess.run([BIN], stdout=subprocess.PIPE, stderr=subprocess.PIPE, timeout=30)
+        return r.returncode == 2   # usage message: the binary runs on this host
+    except Exception:
+        return False
+
+
+def _block(f, payload):
+    n = len(payload)
+    f.write(struct.pack("<i", n))
+    f.write(payload)
+    f.write(struct.pack("<i", n))
+
+
+def write_ic(path, pos, vel, mass, types):
+    """Format-1 IC file; particles must be grouped by type in increasing order."""
+    types = np.asarray(types)
+    assert np.all(np.diff(types) >= 0), "particles must be ordered by type"
+    n = pos.shape[0]
+    npart = [int(np.count_nonzero(types == t)) for t in range(6)]
+    hdr = struct.pack("<6i", *npart)
+    hdr += struct.pack("<6d", *([0.0] * 6))           # masses in the MASS block
+    hdr += struct.pack("<dd", 0.0, 0.0)               # time, redshift
+    hdr += struct.pack("<ii", 0, 0)                   # flag_sfr, flag_feedback
+    hdr += struct.pack("<6I", *npart)                 # npartTotal
+    hdr += struct.pack("<ii", 0, 1)                   # flag_cooling, num_files
+    hdr += struct.pack("<dddd", 0.0, 0.0, 0.0, 1.0)   # BoxSize, OmegaMatter, OmegaLambda, HubbleParam
+    hdr += struct.pack("<ii", 0, 0)                   # flag_stellarage, flag_metals
+    hdr += struct.pack("<6I", *([0] * 6))             # npartTotalHighWord
+    hdr += struct.pack("<iii", 0, 1, 0)               # entropy flag, flag_doubleprecision, flag_ic_info
+    hdr += struct.pack("<f", 0.0)
+    hdr += b"\0" * (256 - len(hdr))
+    assert len(hdr) == 256
+    with open(path, "wb") as f:
+        _block(f, hdr)
+        _block(f, np.ascontiguousarray(pos, dtype="<f8").tobytes())
+        _block(f, np.ascontiguousarray(vel, dtype="<f8").tobytes())
+        _block(f, np.arange(1, n + 1, dtype="<u4").tobytes())
+        _block(f, np.ascontiguousarray(mass, dtype="<f8").tobytes())
+
+
+PARAMS = """InitCondFile {ic}
+OutputDir {out}
+SnapshotFileBase snap
+RestartFile restart
+ResubmitOn 0
+ResubmitCommand none
+OutputListFilename none
+OutputListOn 0
+Omega0 0
+OmegaBaryon 0
+OmegaLambda 0
+OmegaRadiation 0
+HubbleParam 1
+BoxSize 0
+MaxMemSize {memmb}
+TimeOfFirstSnapshot 1e10
+CpuTimeBetRestartFile 1e10
+TimeBetStatistics 1e10
+TimeBegin 0
+TimeMax 1
+TimeBetSnapshot 1e10
+UnitVelocity_in_cm_per_s 1
+UnitLength_in_cm 1
+UnitMass_in_g 1
+UnitMagneticField_in_gauss 1
+GravityConstantInternal 1
+TreeDomainUpdateFrequency 0.0
+MaxSizeTimestep 0.01
+MinSizeTimestep 0
+ComovingIntegrationOn 0
+ICFormat 1
+SnapFormat 1
+NumFilesPerSnapshot 1
+NumFilesWrittenInParallel 1
+TimeLimitCPU 1e9
+SofteningGas {eps1}
+SofteningHalo {eps1}
+SofteningDisk {eps2}
+SofteningBulge {eps1}
+SofteningStars {eps1}
+SofteningBndry {eps1}
+SofteningGasMaxPhys {eps1}
+SofteningHaloMaxPhys {eps1}
+SofteningDiskMaxPhys {eps2}
+SofteningBulgeMaxPhys {eps1}
+SofteningStarsMaxPhys {eps1}
+SofteningBndryMaxPhys {eps1}
+BufferSize 200
+PartAllocFactor 2.0
+InitGasTemp 0
+MinGasTemp 0
+DesNumNgb 32
+MaxHsml 1e10
+MinGasHsmlFractional 0
+"""
+
+
+def types_and_eps(h):
+    """Map per-particle kernel radii to GIZMO particle types 1 and 2."""
+    h = np.asarray(h, dtype=np.float64)
+    vals = sorted(np.unique(h).tolist(), reverse=True)
+    if len(vals) > 2:
+        raise ValueError("the reference harness supports at most two softenings")
+    t = np.where(h == vals[0], 1, 2)
+    eps1 = vals[0] / KERNEL_FAC
+    eps2 = (vals[1] if len(vals) > 1 else vals[0]) / KERNEL_FAC
+    return t, eps1, eps2
+
+
+def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeout=3600):
+    """Run the reference: start-up evaluation (BH pass, relative pass) and
+    optional steady-state steps.  Returns dict with acc (pre-G = acc/G with
+    G = 1), pot, oldacc in input order, interaction counts and timings."""
+    pos, mass, h = ic["pos"], ic["mass"], ic["h"]
+    vel = ic.get("vel", np.zeros_like(pos))
+    n = pos.shape[0]
+    t, eps1, eps2 = types_and_eps(h)
+    order = np.argsort(t, kind="stable")   # the file groups particles by type
+    own = workdir is None
+    d = workdir or tempfile.mkdtemp(prefix="gg_ref_")
+    try:
+        icp = os.path.join(d, "ics")
+        write_ic(icp, pos[order], vel[order], mass[order], t[order])
+        os.makedirs(os.path.join(d, "out"), exist_ok=True)
+        memmb = int(1000 + n * 3000 / 1e6)
+        with open(os.path.join(d, "params"), "w") as f:
+            f.write(PARAMS.format(ic=icp, out=os.path.join(d, "out"), memmb=memmb, eps1=repr(eps1), eps2=repr(eps2)))
+        args = [BIN, os.path.join(d, "params"), repr(tol), os.path.join(d, "res.bin")]
+        if steps:
+            args.append(str(steps))
+            if sample is not None:
+                sp = os.path.join(d, "sample.bin")
+                # IDs in the file are positions in the type-ordered file, plus one
+                inv = np.empty(n, np.int64)
+                inv[order] = np.arange(n)
+                (inv[np.asarray(sample)] + 1).astype("<i8").tofile(sp)
+                args.append(sp)
+        env = dict(os.environ)
+        if threads:
+            env["OMP_NUM_THREADS"] = str(threads)
+        t0 = time.perf_counter()
+        r = subprocess.run(args, cwd=d, stdout=subprocess.PIPE, stderr=subprocess.PIPE, env=env, timeout=timeout)
+        wall = time.perf_counter() - t0
+        if r.returncode != 0:
+            raise RuntimeError("reference run failed (%d): %s" % (r.returncode, r.stdout.decode()[-2000:] +
+                                                                  r.stderr.decode()[-2000:]))
+        rec = np.fromfile(os.path.join(d, "res.bin"), dtype=np.dtype([("id", "<u8"), ("v", "<f8", 5)]))
+        ids = rec["id"].astype(np.int64) - 1
+        out = np.empty((n, 5))
+        out[order[ids]] = rec["v"]
+        info = {"wall_s": wall, "steps": []}
+        bh = np.fromfile(os.path.join(d, "res.bin.bh"), dtype=rec.dtype)
+        out_bh = np.empty((n, 5))
+        out_bh[order[bh["id"].astype(np.int64) - 1]] = bh["v"]
+        kr = np.fromfile(os.path.join(d, "res.bin.keys"), dtype=np.dtype([("id", "<u8"), ("hi", "<u8"), ("lo", "<u8")]))
+        keys_hi = np.empty(n, np.uint64)
+        keys_lo = np.empty(n, np.uint64)
+        kidx = order[kr["id"].astype(np.int64) - 1]
+        keys_hi[kidx], keys_lo[kidx] = kr["hi"], kr["lo"]
+        for line in r.stdout.decode().splitlines():
+            if line.startswith("domain"):
+                kv = dict(p.split("=", 1) for p in line.split()[1:])
+                info["domain"] = {"corner": [float(x) for x in kv["corner"].split(",")], "len": float(kv["len"])}
+            if line.startswith("startup") or line.startswith("step"):
+                kv = dict(p.split("=", 1) for p in line.split()[1 if line.startswith("startup") else 2:] if "=" in p)
+                kv = {k: float(v) for k, v in kv.items()}
+                if line.startswith("startup"):
+                    info["startup"] = kv
+                else:
+                    info["steps"].append(kv)
+        return {"acc": out[:, :3], "pot": out[:, 3], "oldacc": out[:, 4], "acc_bh": out_bh[:, :3],
+                "pot_bh": out_bh[:, 3], "key_hi": keys_hi, "key_lo": keys_lo, "info": info}
+    finally:
+        if own:
+            import shutil
+            shutil.rmtree(d, ignore_errors=True)
+
+
+def rate(ic, seconds=15.0, seed=1, tol=0.0025, threads=None):
+    """Reference particles/s for one steady-state step (domain decomposition +
+    tree build + relative walk of every particle), from a bounded sample: the
+    walk is timed on a seeded random subset of active targets and scaled."""
+    n = ic["pos"].shape[0]
+    cores = threads or os.cpu_count() or 1
+    rng = np.random.default_rng(seed)
+    ns = min(n, 2048)
+    res = None
+    for _ in range(4):
+        sample = np.sort(rng.choice(n, ns, replace=False))
+        res = run(ic, tol=tol, steps=2, sample=sample, threads=cores)
+        st = res["info"]["steps"][-1]
+        t_walk = st["t_gravity"] - st["t_build"]
+        if t_walk > 0.2 * seconds or ns >= n:
+            break
+        ns = min(n, int(ns * max(2.0, 0.3 * seconds / max(t_walk, 1e-3))))
+    per = t_walk / ns
+    step = st["t_domain"] + st["t_build"] + per * n
+    return {"value": n / step, "unit": "particles/s", "cores": cores, "kind": "reference",
+            "sample": "GIZMO's own domain_Decomposition + gravity_tree (compiled reference, FP64, OpenMP %d "
+                      "threads): full keys/sort/tree build + relative walk of %d seeded random active targets of "
+                      "%d, walk time scaled to all targets" % (cores, ns, n),
+            "t_domain_s": st["t_domain"], "t_build_s": st["t_build"], "t_walk_per_particle_us": per * 1e6,
+            "interactions_per_target": st["cost"] / ns}
