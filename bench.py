@@ -212,7 +212,8 @@ def main():
     ic = gen(SEEDS[args.workload] + 7919 * rank)   # independent system per rank
     n = ic["pos"].shape[0]
     dev = torch.device("cuda", local)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream(device=dev)   # every kernel and event of the bench goes on this stream
+    torch.cuda.set_stream(stream)
     rec = ggb200.make_records(ic["pos"], ic["mass"], ic["h"])
     d_rec = torch.from_numpy(rec.view(np.uint8)).to(dev)
     d_acc = torch.empty((n, 3), dtype=torch.float64, device=dev)

@@ -166,7 +166,7 @@ extern "C" gg_status gg_create(const gg_config *cfg, gg_ctx **out)
     for (int i = 0; i < 8; i++) cudaEventCreate(&ctx->ev[i]);
     ctx->have_events = true;
     memset(&ctx->last, 0, sizeof ctx->last);
-    if ((st = ctx->err.ensure(8)) || (st = ctx->counters.ensure(8)) || (st = ctx->inter.ensure(2))) {
+    if ((st = ctx->err.ensure(8)) || (st = ctx->counters.ensure(8)) || (st = ctx->inter.ensure(4))) {
         gg_destroy(ctx);
         return st;
     }
@@ -200,7 +200,7 @@ extern "C" gg_status gg_destroy(gg_ctx *c)
 extern "C" gg_status gg_set_stream(gg_ctx *c, void *s)
 {
     if (!c) return GG_ERR_INVALID;
-    c->stream = s ? (cudaStream_t)s : c->own_stream;
+    c->stream = (cudaStream_t)s;   // NULL is the legacy default stream, as for any CUDA call
     return GG_OK;
 }
 
@@ -418,7 +418,7 @@ static gg_status run_walk(gg_ctx *c, const int *d_active, int n_active, const do
     }
     gg_launch_groups(toff, S, c->cfg.group_size, c->groups.p, c->ngroups.p, c->gscan.p, s);
     GG_CUDA_TRY(cudaMemsetAsync(c->counters.p, 0, 8 * sizeof(int), s));
-    GG_CUDA_TRY(cudaMemsetAsync(c->inter.p, 0, 2 * sizeof(unsigned long long), s));
+    GG_CUDA_TRY(cudaMemsetAsync(c->inter.p, 0, 4 * sizeof(unsigned long long), s));
     WalkParams p;
     p.nodes = c->nodes.p;
     p.parts = c->part.p;
@@ -453,15 +453,18 @@ static gg_status run_walk(gg_ctx *c, const int *d_active, int n_active, const do
 static gg_status collect_stats(gg_ctx *c, gg_stats *out)
 {
     int err[8];
-    unsigned long long inter = 0;
+    unsigned long long inter4[4] = {0, 0, 0, 0};
     int nn = 0, ng = 0;
     GG_CUDA_TRY(cudaMemcpyAsync(err, c->err.p, sizeof err, cudaMemcpyDeviceToHost, c->stream));
-    GG_CUDA_TRY(cudaMemcpyAsync(&inter, c->inter.p, sizeof inter, cudaMemcpyDeviceToHost, c->stream));
+    GG_CUDA_TRY(cudaMemcpyAsync(inter4, c->inter.p, sizeof inter4, cudaMemcpyDeviceToHost, c->stream));
     if (c->t_nnodes.p) GG_CUDA_TRY(cudaMemcpyAsync(&nn, c->t_nnodes.p, sizeof nn, cudaMemcpyDeviceToHost, c->stream));
     if (c->ngroups.p) GG_CUDA_TRY(cudaMemcpyAsync(&ng, c->ngroups.p, sizeof ng, cudaMemcpyDeviceToHost, c->stream));
     GG_CUDA_TRY(cudaStreamSynchronize(c->stream));
     gg_stats &L = c->last;
-    L.interactions = (int64_t)inter;
+    L.interactions = (int64_t)inter4[0];
+    L.far_entries = (int64_t)inter4[1];
+    L.near_entries = (int64_t)inter4[2];
+    L.nodes_tested = (int64_t)inter4[3];
     L.n_nodes = nn;
     L.n_groups = ng;
     L.error_word = err[0];

@@ -45,7 +45,7 @@ struct WalkParams {
     double *acc;                // 3 per output slot
     double *pot;                // per output slot, may be NULL
     int *ninter;                // per output slot, may be NULL
-    unsigned long long *interactions;
+    unsigned long long *interactions;   // [0] interactions, [1] far / [2] near list entries, [3] nodes tested
     int *group_counter;
     int *stack;
     int stack_cap;

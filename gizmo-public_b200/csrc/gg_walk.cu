@@ -75,19 +75,31 @@ struct Kahan {
     __device__ __forceinline__ double value() const { return (double)s - (double)c; }
 };
 
-// cubic-spline softened force and potential factors for u = r/h < 1
-// (kernel.h:452-470); returns w_force, writes w_pot; both still to be scaled
-// by hinv^3 and hinv.
-__device__ __forceinline__ float spline_wf(float u, float *wp)
+// Cubic-spline softened force and potential factors for u = r/h < 1
+// (kernel.h:452-470).  The two pieces (u < 0.5 and 0.5 <= u < 1) are written
+// as one polynomial in u plus 1/u terms whose coefficients are selected by the
+// piece, so lanes on different pieces do not diverge:
+//   w_force = c0 + c1 u + c2 u^2 + c3 u^3 + c4 / u^3
+//   w_pot   = d0 + d1 / u + d2 u^2 + d3 u^3 + d4 u^4 + d5 u^5
+// iu = 1/u is passed in (the caller has it from r^-1 for free).  Returns
+// w_force, writes w_pot; they are still to be scaled by h^-3 and h^-1.
+__device__ __forceinline__ float spline_wf(float u, float iu, float *wp)
 {
-    float u2 = u * u;
-    if (u < 0.5f) {
-        *wp = -2.8f + u2 * (5.333333333333f + u2 * (6.4f * u - 9.6f));
-        return 10.666666666667f + u2 * (32.0f * u - 38.4f);
-    }
-    float iu = 1.0f / u;
-    *wp = -3.2f + 0.066666666667f * iu + u2 * (10.666666666667f + u * (-16.0f + u * (9.6f - 2.133333333333f * u)));
-    return 21.333333333333f - 48.0f * u + 38.4f * u2 - 10.666666666667f * u2 * u - 0.066666666667f * iu * iu * iu;
+    const bool in = u < 0.5f;
+    const float c0 = in ? 10.666666666667f : 21.333333333333f;
+    const float c1 = in ? 0.0f : -48.0f;
+    const float c2 = in ? -38.4f : 38.4f;
+    const float c3 = in ? 32.0f : -10.666666666667f;
+    const float c4 = in ? 0.0f : -0.066666666667f;
+    const float d0 = in ? -2.8f : -3.2f;
+    const float d1 = in ? 0.0f : 0.066666666667f;
+    const float d2 = in ? 5.333333333333f : 10.666666666667f;
+    const float d3 = in ? 0.0f : -16.0f;
+    const float d4 = in ? -9.6f : 9.6f;
+    const float d5 = in ? 6.4f : -2.133333333333f;
+    const float u2 = u * u, iu3 = iu * iu * iu;
+    *wp = fmaf(d1, iu, fmaf(u2, fmaf(u, fmaf(u, fmaf(u, d5, d4), d3), d2), d0));
+    return fmaf(c4, iu3, fmaf(u, fmaf(u, fmaf(u, c3, c2), c1), c0));
 }
 
 template <int TPL>
@@ -153,10 +165,11 @@ __device__ __forceinline__ void flush_near(const float4 *__restrict__ nearE, con
                     fac = mr * rinv * rinv;
                     fpot = -mr;
                 } else {
-                    float hinv = 1.0f / hg;
+                    float hinv = __fdividef(1.0f, hg);
                     float u = r2 * rinv * hinv;
+                    float iu = hg * rinv;
                     float wp;
-                    float wf = spline_wf(u, &wp);
+                    float wf = spline_wf(u, iu, &wp);
                     fac = e.w * wf * hinv * hinv * hinv;
                     fpot = e.w * wp * hinv;
                 }
@@ -272,6 +285,7 @@ __global__ void __launch_bounds__(WALK_THREADS) k_walk(WalkParams p)
 
         // ---- traversal
         int sp = 1, nf = 0, nn = 0;
+        long long list_far = 0, list_near = 0, tested = 0;   // warp-uniform statistics
         bool overflow = false;
         if (lane == 0) stack[0] = grp.root;
         __syncwarp();
@@ -282,6 +296,7 @@ __global__ void __launch_bounds__(WALK_THREADS) k_walk(WalkParams p)
             if (lane < k) node = stack[base + lane];
             __syncwarp();
             sp = base;
+            tested += k;
 
             int act = 0, na = 0, nb = 0;
             bool isfar = false;
@@ -340,6 +355,8 @@ __global__ void __launch_bounds__(WALK_THREADS) k_walk(WalkParams p)
                 }
                 nf += __popc(mf);
                 nn += __popc(mn);
+                list_far += __popc(mf);
+                list_near += __popc(mn);
                 if (nf >= FL) { flush_far<TPL>(far, nf, T); nf = 0; }
                 if (nn >= FL) { flush_near<TPL>(nearE, nearH, nn, T); nn = 0; }
             }
@@ -404,6 +421,8 @@ __global__ void __launch_bounds__(WALK_THREADS) k_walk(WalkParams p)
                     }
                     nf += __popc(mf);
                     nn += __popc(mn);
+                    list_far += __popc(mf);
+                    list_near += __popc(mn);
                     if (nf >= FL) { flush_far<TPL>(far, nf, T); nf = 0; }
                     if (nn >= FL) { flush_near<TPL>(nearE, nearH, nn, T); nn = 0; }
                 }
@@ -436,7 +455,12 @@ __global__ void __launch_bounds__(WALK_THREADS) k_walk(WalkParams p)
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) mycount += __shfl_xor_sync(FULL, mycount, o);
-        if (lane == 0) atomicAdd(p.interactions, (unsigned long long)mycount);
+        if (lane == 0) {
+            atomicAdd(p.interactions, (unsigned long long)mycount);
+            atomicAdd(p.interactions + 1, (unsigned long long)list_far);
+            atomicAdd(p.interactions + 2, (unsigned long long)list_near);
+            atomicAdd(p.interactions + 3, (unsigned long long)tested);
+        }
     }
 }
 

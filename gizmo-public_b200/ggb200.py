@@ -57,7 +57,8 @@ class Domain(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [("interactions", ctypes.c_int64), ("n_nodes", ctypes.c_int64), ("n_targets", ctypes.c_int64),
                 ("n_groups", ctypes.c_int32), ("error_word", ctypes.c_int32), ("ms_keys", ctypes.c_double),
-                ("ms_sort", ctypes.c_double), ("ms_build", ctypes.c_double), ("ms_walk", ctypes.c_double)]
+                ("ms_sort", ctypes.c_double), ("ms_build", ctypes.c_double), ("ms_walk", ctypes.c_double),
+                ("far_entries", ctypes.c_int64), ("near_entries", ctypes.c_int64), ("nodes_tested", ctypes.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

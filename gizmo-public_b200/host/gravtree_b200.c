@@ -1,0 +1,127 @@
+/*
+ * gravtree_b200.c -- GIZMO-side host code of the B200 tree-gravity path.
+ *
+ * This file is compiled inside a GIZMO build (it includes GIZMO's allvars.h
+ * and proto.h) with the compile flag GRAVITY_GPU_B200 and linked with
+ * libgizmo_gravity_b200.so.  It replaces, inside gravity_tree()
+ * (gravity/gravtree.c:51-654), the tree construction block (gravtree.c:67-78,
+ * force_treebuild) and the local walk / export loop (gravtree.c:138-457,
+ * force_treeevaluate per active particle), and leaves everything else to the
+ * reference: the post-processing (x G, OldAcc, switch to the relative
+ * criterion, gravtree.c:475-602), kicks, timesteps and the active list.
+ *
+ * Particle data is passed straight out of P[] with its record stride, so
+ * nothing is copied on the host except the per-particle kernel radii
+ * (ForceSoftening_KernelRadius, proto.h:134-155) and the active index list
+ * (the FirstActiveParticle / NextActiveParticle chain, run.c:473-496).
+ * Single MPI rank per GPU.
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+
+#include "allvars.h"
+#include "proto.h"
+
+#include "gizmo_gravity_b200.h"
+
+static gg_ctx *gg_tree_ctx = NULL;
+static double *gg_soft = NULL, *gg_oldacc = NULL, *gg_acc = NULL, *gg_pot = NULL;
+static int32_t *gg_active = NULL;
+static long gg_cap = 0;
+
+static void gg_fail(const char *what, gg_status st)
+{
+    printf("B200 gravity: %s failed: %s (%d)\n", what, gg_strerror(st), st);
+    endrun(3131);
+}
+
+static void gg_reserve(long n)
+{
+    if (n <= gg_cap) return;
+    gg_cap = n + n / 4 + 1024;
+    gg_soft = (double *)realloc(gg_soft, gg_cap * sizeof(double));
+    gg_oldacc = (double *)realloc(gg_oldacc, gg_cap * sizeof(double));
+    gg_acc = (double *)realloc(gg_acc, 3 * gg_cap * sizeof(double));
+    gg_pot = (double *)realloc(gg_pot, gg_cap * sizeof(double));
+    gg_active = (int32_t *)realloc(gg_active, gg_cap * sizeof(int32_t));
+    if (!gg_soft || !gg_oldacc || !gg_acc || !gg_pot || !gg_active) {
+        printf("B200 gravity: host allocation of %ld entries failed\n", gg_cap);
+        endrun(3132);
+    }
+}
+
+/* Tree construction: replaces force_treebuild(NumPart, NULL) (gravtree.c:74). */
+void gravtree_b200_build(void)
+{
+    gg_status st;
+    int i;
+    if (NTask != 1) {
+        printf("B200 gravity: one MPI rank per GPU (NTask = %d)\n", NTask);
+        endrun(3133);
+    }
+    if (!gg_tree_ctx) {
+        gg_config cfg;
+        gg_config_default(&cfg);
+        if ((st = gg_create(&cfg, &gg_tree_ctx))) gg_fail("gg_create", st);
+    }
+    gg_reserve(NumPart);
+    for (i = 0; i < NumPart; i++) gg_soft[i] = ForceSoftening_KernelRadius(i);
+    int64_t count = NumPart;
+    st = gg_load_particles(gg_tree_ctx, 1, &count, &P[0].Pos[0], (int64_t)sizeof(struct particle_data), &P[0].Mass,
+                           (int64_t)sizeof(struct particle_data), gg_soft, (int64_t)sizeof(double));
+    if (st) gg_fail("gg_load_particles", st);
+    if ((st = gg_build(gg_tree_ctx, NULL))) gg_fail("gg_build", st);
+}
+
+/* Local walk: replaces the force_treeevaluate loop over the active particles
+ * (gravtree.c:138-457).  Leaves the pre-G force and potential in P[] like the
+ * reference's walk does (forcetree.c:2661-2701) and returns the interaction
+ * count (the reference's Costtotal). */
+double gravtree_b200_walk(void)
+{
+    gg_status st;
+    int i;
+    long n = 0;
+    gg_reserve(NumPart);
+    for (i = FirstActiveParticle; i >= 0; i = NextActiveParticle[i]) gg_active[n++] = i;
+    for (i = 0; i < NumPart; i++) gg_oldacc[i] = P[i].OldAcc;
+    gg_stats stats;
+    st = gg_evaluate(gg_tree_ctx, gg_active, n, gg_oldacc, All.ErrTolForceAcc, All.ErrTolTheta, gg_acc, gg_pot, NULL,
+                     &stats);
+    if (st) gg_fail("gg_evaluate", st);
+    for (long k = 0; k < n; k++) {
+        i = gg_active[k];
+        P[i].GravAccel[0] = gg_acc[3 * k];
+        P[i].GravAccel[1] = gg_acc[3 * k + 1];
+        P[i].GravAccel[2] = gg_acc[3 * k + 2];
+#ifdef EVALPOTENTIAL
+        P[i].Potential = gg_pot[k];
+#endif
+    }
+    return (double)stats.interactions;
+}
+
+/* The whole of gravity_tree() for an isolated, tree-only, single-rank run:
+ * build when TreeReconstructFlag is set (gravtree.c:67-78), walk, then the
+ * reference's post-processing for this configuration (gravtree.c:475-522):
+ * switch to the relative criterion, multiply by G, OldAcc = |a|/G. */
+double gravity_tree_b200(void)
+{
+    int i, j;
+    if (TreeReconstructFlag) {
+        gravtree_b200_build();
+        TreeReconstructFlag = 0;
+    }
+    double cost = gravtree_b200_walk();
+    if (All.TypeOfOpeningCriterion == 1) All.ErrTolTheta = 0;
+    for (i = FirstActiveParticle; i >= 0; i = NextActiveParticle[i]) {
+        for (j = 0; j < 3; j++) P[i].GravAccel[j] *= All.G;
+#ifdef EVALPOTENTIAL
+        P[i].Potential *= All.G;
+#endif
+        double ax = P[i].GravAccel[0], ay = P[i].GravAccel[1], az = P[i].GravAccel[2];
+        P[i].OldAcc = sqrt(ax * ax + ay * ay + az * az) / All.G;
+    }
+    return cost;
+}

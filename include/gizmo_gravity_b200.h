@@ -76,6 +76,9 @@ typedef struct gg_stats {
     double ms_sort;
     double ms_build;        /* permute + tree + moments */
     double ms_walk;
+    int64_t far_entries;    /* interaction-list entries evaluated without softening (all groups) */
+    int64_t near_entries;   /* entries that needed the softening branch */
+    int64_t nodes_tested;   /* node opening tests */
 } gg_stats;
 
 typedef struct gg_ctx gg_ctx;
@@ -85,7 +88,8 @@ void gg_config_default(gg_config *cfg);
 gg_status gg_create(const gg_config *cfg, gg_ctx **out);
 gg_status gg_destroy(gg_ctx *ctx);
 const char *gg_strerror(gg_status s);
-/* run this context's work on an existing cudaStream_t (NULL: the ctx's own) */
+/* run this context's work on the given cudaStream_t from now on; NULL selects
+ * the CUDA legacy default stream.  A new context runs on a stream of its own. */
 gg_status gg_set_stream(gg_ctx *ctx, void *cuda_stream);
 gg_status gg_synchronize(gg_ctx *ctx);
 

@@ -15,7 +15,7 @@ CC=/usr/bin/gcc
 # x86-64-v3 (AVX2/FMA): the binary runs on the GPU hosts as well as here
 CFLAGS="-O3 -march=x86-64-v3 -fopenmp -std=gnu99 -w"
 if [ ! -d "$REF" ]; then echo "reference tree not found: $REF" >&2; exit 1; fi
-if [ -x "$OUT/gizmo_ref" ] && [ "$OUT/gizmo_ref" -nt "$HERE/ref_main.c" ] && [ "$OUT/gizmo_ref" -nt "$0" ]; then
+if [ -x "$OUT/gizmo_ref" ] && [ -x "$OUT/gizmo_b200" ] && [ "$OUT/gizmo_b200" -nt "$HERE/ref_main.c" ] && [ "$OUT/gizmo_b200" -nt "$0" ] && [ "$OUT/gizmo_b200" -nt "$HERE/../gizmo-public_b200/host/gravtree_b200.c" ]; then
   echo "oracle/_ref/gizmo_ref is up to date"; exit 0
 fi
 MIRROR="$(mktemp -d /tmp/gg_ref_src.XXXXXX)"
@@ -57,3 +57,12 @@ $CC $CFLAGS -I"$HERE/shim" -c "$HERE/shim/mpi_single.c" -o "$OUT/obj/mpi_single.
 $CC $CFLAGS -I"$HERE/shim" -c "$HERE/shim/gsl_shim.c" -o "$OUT/obj/gsl_shim.o"
 $CC $CFLAGS -o "$OUT/gizmo_ref" $OBJS "$OUT/obj/ref_main.o" "$OUT/obj/mpi_single.o" "$OUT/obj/gsl_shim.o" -lm
 echo "built $OUT/gizmo_ref"
+# GIZMO driving the B200 library through its C host code (needs the CUDA library)
+PKG="$(cd "$HERE/../gizmo-public_b200" && pwd)"
+if [ -f "$PKG/libgizmo_gravity_b200.so" ]; then
+  $CC $CFLAGS -DGG_USE_B200 -I"$HERE/shim" -I"$MIRROR" -c "$HERE/ref_main.c" -o "$OUT/obj/ref_main_b200.o"
+  $CC $CFLAGS -I"$HERE/shim" -I"$MIRROR" -I"$PKG/../include" -c "$PKG/host/gravtree_b200.c" -o "$OUT/obj/gravtree_b200.o"
+  $CC $CFLAGS -o "$OUT/gizmo_b200" $OBJS "$OUT/obj/ref_main_b200.o" "$OUT/obj/gravtree_b200.o" \
+      "$OUT/obj/mpi_single.o" "$OUT/obj/gsl_shim.o" -L"$PKG" -lgizmo_gravity_b200 -Wl,-rpath,'$ORIGIN/../../gizmo-public_b200' -lm
+  echo "built $OUT/gizmo_b200"
+fi

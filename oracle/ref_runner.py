@@ -20,14 +20,17 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 BIN = os.path.join(HERE, "_ref", "gizmo_ref")
+# GIZMO driving the B200 library through gizmo-public_b200/host/gravtree_b200.c
+BIN_B200 = os.path.join(HERE, "_ref", "gizmo_b200")
 KERNEL_FAC = 2.8
 
 
-def available():
-    if not os.path.exists(BIN):
+def available(binary=None):
+    binary = binary or BIN
+    if not os.path.exists(binary):
         return False
     try:
-        r = subprocess.run([BIN], stdout=subprocess.PIPE, stderr=subprocess.PIPE, timeout=30)
+        r = subprocess.run([binary], stdout=subprocess.PIPE, stderr=subprocess.PIPE, timeout=30)
         return r.returncode == 2   # usage message: the binary runs on this host
     except Exception:
         return False
@@ -136,7 +139,7 @@ def types_and_eps(h):
     return t, eps1, eps2
 
 
-def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeout=3600):
+def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeout=3600, binary=None):
     """Run the reference: start-up evaluation (BH pass, relative pass) and
     optional steady-state steps.  Returns dict with acc (pre-G = acc/G with
     G = 1), pot, oldacc in input order, interaction counts and timings."""
@@ -154,7 +157,7 @@ def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeou
         memmb = int(1000 + n * 3000 / 1e6)
         with open(os.path.join(d, "params"), "w") as f:
             f.write(PARAMS.format(ic=icp, out=os.path.join(d, "out"), memmb=memmb, eps1=repr(eps1), eps2=repr(eps2)))
-        args = [BIN, os.path.join(d, "params"), repr(tol), os.path.join(d, "res.bin")]
+        args = [binary or BIN, os.path.join(d, "params"), repr(tol), os.path.join(d, "res.bin")]
         if steps:
             args.append(str(steps))
             if sample is not None:
