@@ -381,12 +381,13 @@ static gg_status walk_setup(gg_ctx *c)
     if (!c->walk_blocks) {
         int per_sm = c->cfg.walk_blocks_per_sm;
         if (per_sm <= 0) per_sm = 2;
-        c->walk_blocks = gg_num_sms() * per_sm;
+        if (per_sm > 3) per_sm = 3;
+        c->walk_blocks = per_sm;   // blocks per SM; the grid is that many per SM
     }
     long long maxg = c->N / c->cfg.group_size + c->S + 1;
     if ((st = c->groups.ensure(maxg)) || (st = c->ngroups.ensure(2)) || (st = c->gscan.ensure(c->S + 1)) ||
         (st = c->toff.ensure(c->S + 1)) ||
-        (st = c->stack.ensure((size_t)c->walk_blocks * (gg_walk_threads() / 32) * GG_STACK_CAP)) ||
+        (st = c->stack.ensure((size_t)c->walk_blocks * gg_num_sms() * (gg_walk_threads() / 32) * GG_STACK_CAP)) ||
         (st = c->scan_scratch.ensure(gg_scan_scratch_ints())))
         return st;
     return GG_OK;

@@ -54,7 +54,7 @@ struct WalkParams {
     int flush;
 };
 int gg_walk_smem_bytes(int flush, int tpl);
-void gg_launch_walk(const WalkParams &p, int tpl, int blocks, cudaStream_t st);
+void gg_launch_walk(const WalkParams &p, int tpl, int blocks_per_sm, cudaStream_t st);
 int gg_walk_threads();
 
 // groups of `gs` consecutive targets per system; toff[S+1] target offsets per system

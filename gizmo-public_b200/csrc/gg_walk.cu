@@ -210,8 +210,10 @@ __device__ __forceinline__ int warp_incl_scan(int v, int lane)
     return v;
 }
 
-template <int TPL>
-__global__ void __launch_bounds__(WALK_THREADS) k_walk(WalkParams p)
+// MINB: resident blocks per SM the register allocation must allow (1..3): a
+// tuning knob trading registers (spills) against warps in flight.
+template <int TPL, int MINB>
+__global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
 {
     extern __shared__ float4 walk_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -464,15 +466,28 @@ __global__ void __launch_bounds__(WALK_THREADS) k_walk(WalkParams p)
     }
 }
 
-void gg_launch_walk(const WalkParams &p, int tpl, int blocks, cudaStream_t st)
+template <int TPL, int MINB>
+static void launch_walk_t(const WalkParams &p, int blocks, int smem, cudaStream_t st)
+{
+    cudaFuncSetAttribute(k_walk<TPL, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k_walk<TPL, MINB><<<blocks, WALK_THREADS, smem, st>>>(p);
+}
+
+// blocks_per_sm selects the register budget of the instantiation (1..3) and
+// the persistent grid is that many blocks per SM
+void gg_launch_walk(const WalkParams &p, int tpl, int blocks_per_sm, cudaStream_t st)
 {
     int smem = gg_walk_smem_bytes(p.flush, tpl);
+    int minb = blocks_per_sm < 1 ? 1 : (blocks_per_sm > 3 ? 3 : blocks_per_sm);
+    int blocks = gg_num_sms() * blocks_per_sm;
     if (tpl == 2) {
-        cudaFuncSetAttribute(k_walk<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        k_walk<2><<<blocks, WALK_THREADS, smem, st>>>(p);
+        if (minb == 1) launch_walk_t<2, 1>(p, blocks, smem, st);
+        else if (minb == 2) launch_walk_t<2, 2>(p, blocks, smem, st);
+        else launch_walk_t<2, 3>(p, blocks, smem, st);
     } else {
-        cudaFuncSetAttribute(k_walk<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        k_walk<1><<<blocks, WALK_THREADS, smem, st>>>(p);
+        if (minb == 1) launch_walk_t<1, 1>(p, blocks, smem, st);
+        else if (minb == 2) launch_walk_t<1, 2>(p, blocks, smem, st);
+        else launch_walk_t<1, 3>(p, blocks, smem, st);
     }
     gg_note_launches(1);
 }
