@@ -110,6 +110,7 @@ def load_library():
             "gg_radix_sort_pairs": (i32, [i64, P, P, i32, P]),
             "gg_direct_sum_fp64": (i32, [i64, P, P, P, i64, P, P, P, P]),
             "gg_fp32_peak_probe": (i32, [ctypes.POINTER(dbl), P]),
+            "gg_radix_sort_pairs_noalloc": (i32, [i64, P, P, i32, P]),
             "gg_kernel_launches": (i64, []),
         }
         for name, (res, args) in sig.items():
@@ -282,6 +283,16 @@ def peano_hilbert_keys(d_pos, n, domain, d_keys, stream=None):
 def radix_sort_pairs(d_keys, d_vals, n, key_bits=64, stream=None):
     lib = load_library()
     _check(lib.gg_radix_sort_pairs(n, _ptr(d_keys), _ptr(d_vals), key_bits, stream), "gg_radix_sort_pairs")
+
+
+NOALLOC_SORT_MAX_N = 1 << 20
+
+
+def radix_sort_pairs_noalloc(d_keys, d_vals, n, key_bits=64, stream=None):
+    """Radix sort that uses the library's static device scratch (no allocation)."""
+    lib = load_library()
+    _check(lib.gg_radix_sort_pairs_noalloc(n, _ptr(d_keys), _ptr(d_vals), key_bits, stream),
+           "gg_radix_sort_pairs_noalloc")
 
 
 def direct_sum_fp64(d_pos, d_mass, d_h, n_src, d_targets, n_tgt, d_acc, d_pot, stream=None):

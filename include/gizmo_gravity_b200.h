@@ -138,6 +138,21 @@ gg_status gg_peano_hilbert_keys(int64_t n, const double *d_pos, const gg_domain 
 /* stable LSD radix sort of (key, value) pairs, replacing mysort_peano
  * (peano.c:414-462); key_bits <= 64; scratch is allocated by the call */
 gg_status gg_radix_sort_pairs(int64_t n, uint64_t *d_keys, uint32_t *d_vals, int32_t key_bits, void *stream);
+/* The same stable radix sort without any device allocation.  It has no
+ * counterpart in the reference (whose sort runs on the host).  It is for
+ * callers that cannot allocate device memory: a process whose device memory
+ * is already reserved in full by another allocator (a framework's caching
+ * allocator, a serving loop admitting work against a fixed memory budget)
+ * would see cudaMalloc fail or bypass its accounting, and a latency-critical
+ * loop cannot take cudaFree's implicit device synchronisation.  The scratch is
+ * one static device array of the library (about 16 MB, held by every GPU that
+ * loads the library until the process exits), so n is limited to
+ * GG_NOALLOC_SORT_MAX_N; larger n returns GG_ERR_TOO_LARGE.  The first call on
+ * a device looks up the array's device address; make that first call before
+ * any stream capture.  All calls share the array: calls whose work overlaps
+ * on the GPU race and must not be issued.  Blocking (synchronises `stream`). */
+#define GG_NOALLOC_SORT_MAX_N (1 << 20)
+gg_status gg_radix_sort_pairs_noalloc(int64_t n, uint64_t *d_keys, uint32_t *d_vals, int32_t key_bits, void *stream);
 /* FP64 direct summation over all sources with the walk's pair rule (the
  * reference declares force_treeevaluate_direct, gravity/forcetree.h:76, but
  * ships no definition); used to measure force errors at full size */
