@@ -77,6 +77,12 @@ struct gg_ctx {
     DevBuf<GGPart> in_rec, part;
     DevBuf<GGDomainDev> dom;
     DevBuf<unsigned long long> extent_mm;
+    DevBuf<unsigned> hmm;          // per system [min h, max h] as float bits
+    bool h_mixed = false;          // some system holds several kernel radii: group targets by softening
+    int order_by_softening = 1;    // from gg_config.target_order
+    DevBuf<unsigned long long> tkey;
+    DevBuf<unsigned> tval;
+    DevBuf<int> tlist2, tout2;
     DevBuf<unsigned long long> keys;
     DevBuf<unsigned> perm, rank;
     DevBuf<char> sort_scratch;
@@ -158,6 +164,7 @@ extern "C" gg_status gg_create(const gg_config *cfg, gg_ctx **out)
     gg_ctx *ctx = new gg_ctx();
     ctx->cfg = c;
     ctx->device = c.device;
+    ctx->order_by_softening = c.target_order == 1;
     gg_status st = set_device(ctx);
     if (st) { delete ctx; return st; }
     cudaError_t e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
@@ -180,7 +187,8 @@ extern "C" gg_status gg_destroy(gg_ctx *c)
     if (!c) return GG_ERR_INVALID;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    c->poff.release(); c->in_rec.release(); c->part.release(); c->dom.release(); c->extent_mm.release();
+    c->poff.release(); c->in_rec.release(); c->part.release(); c->dom.release(); c->extent_mm.release(); c->hmm.release(); c->tkey.release(); c->tval.release();
+    c->tlist2.release(); c->tout2.release();
     c->keys.release(); c->perm.release(); c->rank.release(); c->sort_scratch.release();
     c->t_start.release(); c->t_end.release(); c->t_level.release(); c->t_parent.release(); c->t_sys.release();
     c->t_nch.release(); c->t_child.release(); c->t_counter.release(); c->t_bnd.release(); c->t_depth.release();
@@ -233,7 +241,7 @@ static gg_status set_systems(gg_ctx *c, int S, const int64_t *counts)
     if ((st = c->poff.ensure(S + 1))) return st;
     GG_CUDA_TRY(cudaMemcpyAsync(c->poff.p, poff.data(), (S + 1) * sizeof(int), cudaMemcpyHostToDevice, c->stream));
     if ((st = c->in_rec.ensure(N)) || (st = c->part.ensure(N)) || (st = c->dom.ensure(S)) ||
-        (st = c->extent_mm.ensure((size_t)S * 6)) || (st = c->keys.ensure(N)) || (st = c->perm.ensure(N)) ||
+        (st = c->extent_mm.ensure((size_t)S * 6)) || (st = c->hmm.ensure((size_t)S * 2)) || (st = c->keys.ensure(N)) || (st = c->perm.ensure(N)) ||
         (st = c->rank.ensure(N)) || (st = c->oldacc.ensure(N)))
         return st;
     return GG_OK;
@@ -261,7 +269,8 @@ extern "C" gg_status gg_load_particles(gg_ctx *c, int32_t S, const int64_t *coun
     GG_CUDA_TRY(cudaStreamSynchronize(c->stream));   // staging buffer may still feed a previous copy
     const char *pb = (const char *)pos, *mb = (const char *)mass, *hb = (const char *)soft_h;
     GGPart *dst = c->h_stage;
-#pragma omp parallel for schedule(static)
+    int mixed = 0;
+#pragma omp parallel for schedule(static) reduction(| : mixed)
     for (long long i = 0; i < N; i++) {
         const double *x = (const double *)(pb + i * pos_stride);
         GGPart r;
@@ -269,7 +278,11 @@ extern "C" gg_status gg_load_particles(gg_ctx *c, int32_t S, const int64_t *coun
         r.m = (float)*(const double *)(mb + i * mass_stride);
         r.h = (float)*(const double *)(hb + i * soft_stride);
         dst[i] = r;
+        if (i > 0 && r.h != (float)*(const double *)(hb + (i - 1) * soft_stride)) mixed = 1;
     }
+    // a change of kernel radius between neighbouring particles of different
+    // systems also counts: harmless (ordering then just keeps each system's order)
+    c->h_mixed = mixed != 0;
     if (N) GG_CUDA_TRY(cudaMemcpyAsync(c->in_rec.p, c->h_stage, N * sizeof(GGPart), cudaMemcpyHostToDevice, c->stream));
     return GG_OK;
 }
@@ -280,8 +293,17 @@ extern "C" gg_status gg_load_particles_device(gg_ctx *c, int32_t S, const int64_
     gg_status st;
     if ((st = set_device(c))) return st;
     if ((st = set_systems(c, S, counts))) return st;
-    if (c->N)
+    if (c->N) {
         GG_CUDA_TRY(cudaMemcpyAsync(c->in_rec.p, d_records, c->N * sizeof(GGPart), cudaMemcpyDeviceToDevice, c->stream));
+        // the range of kernel radii decides (once, here) whether walks order targets by softening
+        gg_launch_extent(c->in_rec.p, (int)c->N, c->poff.p, S, c->extent_mm.p, c->hmm.p, c->dom.p, c->err.p, c->stream);
+        std::vector<unsigned> h(2 * (size_t)S);
+        GG_CUDA_TRY(cudaMemcpyAsync(h.data(), c->hmm.p, h.size() * sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+        GG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        c->h_mixed = false;
+        for (int s = 0; s < S; s++)
+            if (h[2 * s] != h[2 * s + 1] && h[2 * s] != 0x7f800000u) c->h_mixed = true;
+    }
     return GG_OK;
 }
 
@@ -344,7 +366,7 @@ extern "C" gg_status gg_build(gg_ctx *c, const gg_domain *domains)
         GG_CUDA_TRY(cudaMemcpyAsync(c->dom.p, d.data(), S * sizeof(GGDomainDev), cudaMemcpyHostToDevice, s));
         GG_CUDA_TRY(cudaStreamSynchronize(s));
     } else if (N > 0) {
-        gg_launch_extent(c->in_rec.p, N, c->poff.p, S, c->extent_mm.p, c->dom.p, c->err.p, s);
+        gg_launch_extent(c->in_rec.p, N, c->poff.p, S, c->extent_mm.p, c->hmm.p, c->dom.p, c->err.p, s);
     }
     if (N > 0) gg_launch_keys(c->in_rec.p, N, c->poff.p, S, c->dom.p, c->keys.p, c->perm.p, c->err.p, s);
     if (timing) cudaEventRecord(c->ev[1], s);
@@ -412,6 +434,17 @@ static gg_status run_walk(gg_ctx *c, const int *d_active, int n_active, const do
         tlist = c->tlist.p;
         tout = c->tout.p;
         toff = c->toff.p;
+    }
+    if (c->h_mixed && c->order_by_softening) {
+        const int nt = d_active ? n_active : N;
+        if ((st = c->tkey.ensure(nt)) || (st = c->tval.ensure(nt)) || (st = c->tlist2.ensure(nt)) ||
+            (st = c->tout2.ensure(nt)))
+            return st;
+        st = gg_order_targets_by_softening(nt, tlist, tout, c->part.p, c->poff.p, S, c->tkey.p, c->tval.p,
+                                           c->tlist2.p, tout ? c->tout2.p : nullptr, c->sort_scratch.p, c->err.p, s);
+        if (st) return st;
+        tlist = c->tlist2.p;
+        if (tout) tout = c->tout2.p;
     }
     if (d_old_acc) {
         GG_CUDA_TRY(cudaMemcpyAsync(c->oldacc.p, d_old_acc, (size_t)N * sizeof(double), cudaMemcpyDeviceToDevice, s));

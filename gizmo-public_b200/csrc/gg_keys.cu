@@ -21,50 +21,70 @@ __device__ __forceinline__ int gg_sys_of(const int *__restrict__ poff, int S, in
     return lo;
 }
 
-__global__ void k_extent_init(unsigned long long *mm, int S)
+__global__ void k_extent_init(unsigned long long *mm, unsigned *hmm, int S)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < S * 6) mm[t] = (t % 6) < 3 ? ~0ull : 0ull;   // [min x,y,z | max x,y,z] in ordered encoding
+    if (hmm && t < S * 2) hmm[t] = (t & 1) ? 0u : 0x7f800000u;
 }
 
-// Each thread scans a contiguous run of particles and flushes its running
-// min/max with 64-bit atomics whenever the system changes: order-independent,
-// so the result is exact and deterministic.
+// Each warp reduces a contiguous chunk of particles, reading it coalesced
+// (lane l takes every 32nd record), one system segment at a time, and flushes
+// the segment's min/max with 64-bit atomics on an order-preserving encoding:
+// order-independent, so the result is exact and deterministic.  The per-system
+// range of kernel radii (positive floats, ordered as their bit patterns) goes
+// to hmm[2s], hmm[2s+1].
+#define EXTENT_CHUNK 4096
 __global__ void k_extent(const GGPart *__restrict__ rec, int n, const int *__restrict__ poff, int S,
-                         unsigned long long *mm, int *err)
+                         unsigned long long *mm, unsigned *hmm, int *err)
 {
-    int nthreads = gridDim.x * blockDim.x;
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    int per = (n + nthreads - 1) / nthreads;
-    int i0 = t * per, i1 = min(n, i0 + per);
-    if (i0 >= i1) return;
-    int s = gg_sys_of(poff, S, i0), send = __ldg(poff + s + 1);
-    double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
     bool bad = false;
-    for (int i = i0; i < i1; i++) {
-        while (i >= send) {
-            if (mn[0] <= mx[0])
+    for (long long c0 = (long long)warp * EXTENT_CHUNK; c0 < n; c0 += (long long)nwarps * EXTENT_CHUNK) {
+        const int cb = (int)c0, ce = (int)min((long long)n, c0 + EXTENT_CHUNK);
+        int s = gg_sys_of(poff, S, cb);
+        for (int seg = cb; seg < ce; s++) {
+            const int se = min(ce, __ldg(poff + s + 1));
+            double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+            float hmin = INFINITY, hmax = 0.f;
+            for (int i = seg + lane; i < se; i += 32) {
+                GGPart p = rec[i];
+                double v[3] = {p.x, p.y, p.z};
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    if (!isfinite(v[k])) bad = true;
+                    mn[k] = fmin(mn[k], v[k]);
+                    mx[k] = fmax(mx[k], v[k]);
+                }
+                hmin = fminf(hmin, p.h);
+                hmax = fmaxf(hmax, p.h);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    mn[k] = fmin(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+                    mx[k] = fmax(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+                }
+                hmin = fminf(hmin, __shfl_xor_sync(0xffffffffu, hmin, o));
+                hmax = fmaxf(hmax, __shfl_xor_sync(0xffffffffu, hmax, o));
+            }
+            if (lane == 0 && se > seg) {
+#pragma unroll
                 for (int k = 0; k < 3; k++) {
                     atomicMin(&mm[s * 6 + k], gg_dbl_to_ordered(mn[k]));
                     atomicMax(&mm[s * 6 + 3 + k], gg_dbl_to_ordered(mx[k]));
                 }
-            for (int k = 0; k < 3; k++) { mn[k] = INFINITY; mx[k] = -INFINITY; }
-            s++;
-            send = __ldg(poff + s + 1);
-        }
-        GGPart p = rec[i];
-        double v[3] = {p.x, p.y, p.z};
-        for (int k = 0; k < 3; k++) {
-            if (!isfinite(v[k])) bad = true;
-            mn[k] = fmin(mn[k], v[k]);
-            mx[k] = fmax(mx[k], v[k]);
+                if (hmm) {
+                    atomicMin(&hmm[2 * s], __float_as_uint(fmaxf(hmin, 0.f)));
+                    atomicMax(&hmm[2 * s + 1], __float_as_uint(fmaxf(hmax, 0.f)));
+                }
+            }
+            seg = se;
         }
     }
-    if (mn[0] <= mx[0])
-        for (int k = 0; k < 3; k++) {
-            atomicMin(&mm[s * 6 + k], gg_dbl_to_ordered(mn[k]));
-            atomicMax(&mm[s * 6 + 3 + k], gg_dbl_to_ordered(mx[k]));
-        }
     if (bad) atomicOr(err, GG_EBIT_BAD_INPUT);
 }
 
@@ -158,14 +178,15 @@ __global__ void k_keys_plain(const double *__restrict__ pos, long long n, GGDoma
     if (bad && err) atomicOr(err, GG_EBIT_BAD_INPUT);
 }
 
-void gg_launch_extent(const GGPart *rec, int n, const int *poff, int S, unsigned long long *mm, GGDomainDev *dom,
-                      int *err, cudaStream_t st)
+void gg_launch_extent(const GGPart *rec, int n, const int *poff, int S, unsigned long long *mm, unsigned *hmm,
+                      GGDomainDev *dom, int *err, cudaStream_t st)
 {
-    k_extent_init<<<(S * 6 + 255) / 256, 256, 0, st>>>(mm, S);
+    k_extent_init<<<(S * 6 + 255) / 256, 256, 0, st>>>(mm, hmm, S);
     int threads = 256, blocks = gg_num_sms() * 4;
-    if ((long long)blocks * threads > n) blocks = (n + threads - 1) / threads;
+    long long chunks = ((long long)n + EXTENT_CHUNK - 1) / EXTENT_CHUNK;
+    if ((long long)blocks * (threads / 32) > chunks) blocks = (int)((chunks + (threads / 32) - 1) / (threads / 32));
     if (blocks < 1) blocks = 1;
-    k_extent<<<blocks, threads, 0, st>>>(rec, n, poff, S, mm, err);
+    k_extent<<<blocks, threads, 0, st>>>(rec, n, poff, S, mm, hmm, err);
     k_extent_finalize<<<(S + 127) / 128, 128, 0, st>>>(mm, S, dom);
     gg_note_launches(3);
 }

@@ -303,3 +303,51 @@ extern "C" gg_status gg_fp32_peak_probe(double *tflops, void *stream)
     *tflops = best;
     return GG_OK;
 }
+
+// ---- walk targets ordered by (system, softening) -------------------------------
+// Groups of targets that share a kernel radius keep the near field (entries
+// within the group's largest softening) as small as the targets need; in a
+// halo + disk system a group mixing the two would give its disk targets the
+// halo's larger near zone.  Within a class the targets stay in key order.
+__global__ void k_target_keys(int nt, const int *__restrict__ tlist, const GGPart *__restrict__ parts,
+                              const int *__restrict__ poff, int S, unsigned long long *key, unsigned *val)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+        int pi = tlist ? tlist[t] : t;
+        int lo = 0, hi = S - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (__ldg(poff + mid) <= pi) lo = mid; else hi = mid - 1;
+        }
+        key[t] = ((unsigned long long)lo << 32) | __float_as_uint(fmaxf(parts[pi].h, 0.f));
+        val[t] = (unsigned)t;
+    }
+}
+
+__global__ void k_target_apply(int nt, const unsigned *__restrict__ val, const int *__restrict__ tlist_in,
+                               const int *__restrict__ tout_in, int *tlist_out, int *tout_out)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
+        int t = (int)val[k];
+        tlist_out[k] = tlist_in ? tlist_in[t] : t;
+        if (tout_out) tout_out[k] = tout_in[t];
+    }
+}
+
+gg_status gg_order_targets_by_softening(int nt, const int *tlist_in, const int *tout_in, const GGPart *parts,
+                                        const int *poff, int S, unsigned long long *key, unsigned *val,
+                                        int *tlist_out, int *tout_out, void *sort_scratch, int *err, cudaStream_t st)
+{
+    if (nt <= 0) return GG_OK;
+    int sbits = 0;
+    while ((1 << sbits) < S) sbits++;
+    int np = (32 + sbits + 7) / 8;
+    int blocks = gg_num_sms() * 4;
+    k_target_keys<<<blocks, 256, 0, st>>>(nt, tlist_in, parts, poff, S, key, val);
+    gg_note_launches(1);
+    gg_status s = gg_sort_pairs_run(key, val, nt, np, 0, nullptr, 1, sort_scratch, err, st);
+    if (s) return s;
+    k_target_apply<<<blocks, 256, 0, st>>>(nt, val, tlist_in, tout_in, tlist_out, tout_out);
+    gg_note_launches(1);
+    return GG_OK;
+}

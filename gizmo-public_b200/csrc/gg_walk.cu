@@ -35,12 +35,18 @@
 
 int gg_walk_threads() { return WALK_THREADS; }
 
+// per-warp shared memory in float4 units: far float4[cap], near float4[cap],
+// near (h, 1/h) float2[cap] rounded up to whole float4s; cap = flush + 32
+__host__ __device__ __forceinline__ int walk_warp_float4s(int flush)
+{
+    const int cap = flush + 32;
+    return 2 * cap + (cap + 1) / 2;
+}
+
 int gg_walk_smem_bytes(int flush, int tpl)
 {
     (void)tpl;
-    int cap = flush + 32;
-    // per warp: far float4[cap], near float4[cap], near h float[cap] (rounded up to float4)
-    return WALK_WARPS * (2 * cap + cap / 4 + 1) * 16;
+    return WALK_WARPS * walk_warp_float4s(flush) * 16;
 }
 
 __device__ __forceinline__ GGNode load_node(const GGNode *p)
@@ -104,7 +110,7 @@ __device__ __forceinline__ float spline_wf(float u, float iu, float *wp)
 
 template <int TPL>
 struct Targets {
-    float x[TPL], y[TPL], z[TPL], h[TPL];
+    float x[TPL], y[TPL], z[TPL], h[TPL], hinv[TPL];
     bool valid[TPL];
     Kahan ax[TPL], ay[TPL], az[TPL], pot[TPL];
     int nint[TPL];
@@ -142,16 +148,17 @@ __device__ __forceinline__ void flush_far(const float4 *__restrict__ far, int nf
 }
 
 template <int TPL>
-__device__ __forceinline__ void flush_near(const float4 *__restrict__ nearE, const float *__restrict__ nearH, int nn,
+__device__ __forceinline__ void flush_near(const float4 *__restrict__ nearE, const float2 *__restrict__ nearH, int nn,
                                            Targets<TPL> &T)
 {
     __syncwarp();
     float px[TPL], py[TPL], pz[TPL], pp[TPL];
 #pragma unroll
-    for (int s = 0; s < TPL; s++) { px[s] = 0.f; py[s] = 0.f; pz[s] = 0.f; pp[s] = 0.f; }
+    for (int s = 0; s < TPL; s++) { px[s] = 0.f; py[s] = 0.f; pz[s] = 0.f; pp[s] = 0.f; T.nint[s] += nn; }
     for (int j = 0; j < nn; j++) {
         const float4 e = nearE[j];
-        const float hp = nearH[j];
+        const float2 hh = nearH[j];   // source kernel radius and its inverse
+        const float hp = hh.x;
 #pragma unroll
         for (int s = 0; s < TPL; s++) {
             float dx = e.x - T.x[s], dy = e.y - T.y[s], dz = e.z - T.z[s];
@@ -165,7 +172,7 @@ __device__ __forceinline__ void flush_near(const float4 *__restrict__ nearE, con
                     fac = mr * rinv * rinv;
                     fpot = -mr;
                 } else {
-                    float hinv = __fdividef(1.0f, hg);
+                    float hinv = T.h[s] >= hp ? T.hinv[s] : hh.y;
                     float u = r2 * rinv * hinv;
                     float iu = hg * rinv;
                     float wp;
@@ -177,7 +184,8 @@ __device__ __forceinline__ void flush_near(const float4 *__restrict__ nearE, con
                 py[s] = fmaf(dy, fac, py[s]);
                 pz[s] = fmaf(dz, fac, pz[s]);
                 pp[s] += fpot;
-                T.nint[s] += 1;
+            } else {
+                T.nint[s] -= 1;   // self (or a coincident particle): not an interaction
             }
         }
     }
@@ -219,9 +227,9 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
     const int FL = p.flush, cap = FL + 32;
-    float4 *far = walk_smem + (size_t)warp * (2 * cap + cap / 4 + 1);
+    float4 *far = walk_smem + (size_t)warp * walk_warp_float4s(FL);
     float4 *nearE = far + cap;
-    float *nearH = reinterpret_cast<float *>(nearE + cap);
+    float2 *nearH = reinterpret_cast<float2 *>(nearE + cap);
     int *stack = p.stack + (size_t)(blockIdx.x * WALK_WARPS + warp) * p.stack_cap;
     const int ngroups = *p.ngroups;
     const double theta = p.theta;
@@ -250,6 +258,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
             tpi[s] = -1;
             tx[s] = ty[s] = tz[s] = 0.0;
             T.h[s] = 0.f;
+            T.hinv[s] = INFINITY;
             if (v) {
                 int t = grp.first + k;
                 int pi = p.tlist ? p.tlist[t] : t;
@@ -257,6 +266,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
                 GGPart q = load_part(p.parts + pi);
                 tx[s] = q.x; ty[s] = q.y; tz[s] = q.z;
                 T.h[s] = q.h;
+                T.hinv[s] = q.h > 0.f ? __frcp_rn(q.h) : INFINITY;
                 double oa = p.oldacc_in ? p.oldacc_in[p.perm[pi]] : 0.0;
                 aold_min = fmin(aold_min, p.tol * oa);
                 hmin = fminf(hmin, q.h);
@@ -352,7 +362,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
                     else {
                         int pos = nn + __popc(mn & lt_mask);
                         nearE[pos] = ent;
-                        nearH[pos] = hp;
+                        nearH[pos] = make_float2(hp, hp > 0.f ? __frcp_rn(hp) : INFINITY);
                     }
                 }
                 nf += __popc(mf);
@@ -418,7 +428,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
                         else {
                             int pos = nn + __popc(mn & lt_mask);
                             nearE[pos] = pe;
-                            nearH[pos] = ph;
+                            nearH[pos] = make_float2(ph, ph > 0.f ? __frcp_rn(ph) : INFINITY);
                         }
                     }
                     nf += __popc(mf);

@@ -55,7 +55,9 @@ typedef struct gg_config {
     int32_t flush_threshold;  /* interaction-list entries per flush, 32..128 (default 64) */
     int32_t walk_blocks_per_sm; /* persistent walk blocks per SM, 0 = default */
     int32_t timing;           /* 1: record per-stage device times into gg_stats */
-    int32_t reserved[2];
+    int32_t target_order;     /* 0: walk groups follow key order (default); 1: when a system has
+                                 several kernel radii, groups gather targets of one radius */
+    int32_t reserved[1];
 } gg_config;
 
 /* root cube of one system: domain_findExtent (domain.c:2518-2570) */
