@@ -79,8 +79,20 @@ __device__ __forceinline__ int lower_bound_key(const unsigned long long *__restr
     return lo;
 }
 
-// number of children of node [s,e) at geometric level `lev`
-__device__ __forceinline__ int chunk_children(int cnt, int leaf) { return (cnt + leaf - 1) / leaf; }
+// A full-depth cell with more than `leaf` particles is split into at most 8
+// equal chunks (which split again at the next depth if still too large), so no
+// node ever has more than 8 children.
+__device__ __forceinline__ int chunk_size(int cnt, int leaf)
+{
+    const int n8 = min(8, (cnt + leaf - 1) / leaf);
+    return (cnt + n8 - 1) / n8;
+}
+// every chunk non-empty: ceil(cnt / size) <= 8 chunks of `size` particles (the last may be shorter)
+__device__ __forceinline__ int chunk_children(int cnt, int leaf)
+{
+    const int sz = chunk_size(cnt, leaf);
+    return (cnt + sz - 1) / sz;
+}
 
 // Count phase for one depth: 8 threads per node find the 7 digit boundaries;
 // per-block sums of child counts go to blocksum[blockIdx.x].
@@ -104,8 +116,9 @@ __global__ void __launch_bounds__(TB_THREADS) k_tree_count(int depth, const unsi
         int s = 0, e = 0, lev = 0;
         if (valid) { s = tb.start[k]; e = tb.end[k]; lev = tb.level[k]; }
         const int cnt = e - s;
-        const bool digit_mode = valid && cnt > leaf && lev < GG_MAX_LEVEL;
-        const bool chunk_mode = valid && cnt > leaf && lev >= GG_MAX_LEVEL;
+        const bool split = valid && cnt > leaf && depth < GG_MAX_DEPTH - 1;
+        const bool digit_mode = split && lev < GG_MAX_LEVEL;
+        const bool chunk_mode = split && lev >= GG_MAX_LEVEL;
         int b = s;
         if (digit_mode && j > 0) {
             int shift = 3 * (GG_MAX_LEVEL - (lev + 1));
@@ -212,9 +225,10 @@ __global__ void __launch_bounds__(TB_THREADS) k_tree_write(int depth, const unsi
             if (nch) {
                 int s = tb.start[k], e = tb.end[k], lev = tb.level[k], sys = tb.sys[k];
                 if (lev >= GG_MAX_LEVEL) {
+                    const int csz = chunk_size(e - s, leaf);
                     for (int c = j; c < nch; c += TB_GROUP) {
                         int idx = first + c;
-                        int cs = s + c * leaf, ce2 = min(e, cs + leaf);
+                        int cs = s + c * csz, ce2 = min(e, cs + csz);
                         tb.start[idx] = cs; tb.end[idx] = ce2; tb.level[idx] = GG_CHUNK_LEVEL;
                         tb.parent[idx] = k; tb.sys[idx] = sys; tb.counter[idx] = 0;
                     }

@@ -7,7 +7,7 @@
 
 #define GG_MAX_LEVEL 21          // key levels: 21 bits per dimension, 63-bit keys
 #define GG_CHUNK_LEVEL 22        // leaf chunks below a full-depth cell
-#define GG_MAX_DEPTH 24          // tree depth bound (root + 21 key levels + chunks + slack)
+#define GG_MAX_DEPTH 28          // tree depth bound: root + 21 key levels + chunk levels; the last depth is all leaves
 #define GG_WARP 32
 
 // error bits of the device error word
@@ -16,6 +16,7 @@
 #define GG_EBIT_STACK_OVERFLOW 4
 #define GG_EBIT_BAD_INPUT 8
 #define GG_EBIT_LIST 16
+#define GG_EBIT_WALK_TIMEOUT 32
 
 // One particle, 32 bytes: FP64 position, FP32 mass and kernel radius h.
 struct __align__(32) GGPart {

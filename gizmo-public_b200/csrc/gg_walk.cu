@@ -35,12 +35,16 @@
 
 int gg_walk_threads() { return WALK_THREADS; }
 
-// per-warp shared memory in float4 units: far float4[cap], near float4[cap],
-// near (h, 1/h) float2[cap] rounded up to whole float4s; cap = flush + 32
+// Per-warp shared memory, in float4 units:
+//   far list float4[cap] | near list float4[cap] | near (h, 1/h) float2[cap] |
+//   node stack int[WALK_SSTACK]
+// with cap = flush + 32.  The stack spills to the warp's global stack area
+// when it overflows (deep or wide traversals only).
+#define WALK_SSTACK 512
 __host__ __device__ __forceinline__ int walk_warp_float4s(int flush)
 {
     const int cap = flush + 32;
-    return 2 * cap + (cap + 1) / 2;
+    return 2 * cap + (cap + 1) / 2 + WALK_SSTACK / 4;
 }
 
 int gg_walk_smem_bytes(int flush, int tpl)
@@ -230,7 +234,8 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
     float4 *far = walk_smem + (size_t)warp * walk_warp_float4s(FL);
     float4 *nearE = far + cap;
     float2 *nearH = reinterpret_cast<float2 *>(nearE + cap);
-    int *stack = p.stack + (size_t)(blockIdx.x * WALK_WARPS + warp) * p.stack_cap;
+    int *sstack = reinterpret_cast<int *>(far + 2 * cap + (cap + 1) / 2);
+    int *gstack = p.stack + (size_t)(blockIdx.x * WALK_WARPS + warp) * p.stack_cap;
     const int ngroups = *p.ngroups;
     const double theta = p.theta;
 
@@ -296,26 +301,44 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
         const double hmaxd = (double)hmax, hmind = (double)hmin;
 
         // ---- traversal
-        int sp = 1, nf = 0, nn = 0;
+        // The node stack lives in shared memory (sp entries) on top of a spill
+        // area in global memory (gsp entries).  Each round pops up to 32 nodes;
+        // the next round's node records are loaded before this round's leaf
+        // particles and list flushes are processed, which hides their latency.
+        int sp = 1, gsp = 0, nf = 0, nn = 0;
         long long list_far = 0, list_near = 0, tested = 0;   // warp-uniform statistics
         bool overflow = false;
-        if (lane == 0) stack[0] = grp.root;
+        if (lane == 0) sstack[0] = grp.root;
         __syncwarp();
-        while (sp > 0) {
+        // pop up to 32 nodes (one per lane); returns the count (warp-uniform)
+        auto pop_nodes = [&](int &node) -> int {
+            if (sp == 0 && gsp > 0) {   // refill from the spill area, keeping stack order
+                const int m = min(gsp, WALK_SSTACK / 2);
+                for (int i = lane; i < m; i += 32) sstack[i] = gstack[gsp - m + i];
+                gsp -= m;
+                sp = m;
+                __syncwarp();
+            }
             const int k = min(sp, 32);
-            const int base = sp - k;
-            int node = -1;
-            if (lane < k) node = stack[base + lane];
+            node = -1;
+            if (lane < k) node = sstack[sp - k + lane];
+            sp -= k;
             __syncwarp();
-            sp = base;
+            return k;
+        };
+        int node = -1;
+        int k = pop_nodes(node);
+        GGNode cur;
+        if (lane < k) cur = load_node(p.nodes + node);
+        while (k > 0) {
             tested += k;
 
             int act = 0, na = 0, nb = 0;
             bool isfar = false;
             float4 ent = make_float4(0.f, 0.f, 0.f, 0.f);
             float hp = 0.f;
-            if (node >= 0) {
-                const GGNode nd = load_node(p.nodes + node);
+            if (lane < k) {
+                const GGNode nd = cur;
                 na = nd.a;
                 nb = nd.b;
                 if (nd.mass > 0.f) {
@@ -369,23 +392,39 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
                 nn += __popc(mn);
                 list_far += __popc(mf);
                 list_near += __popc(mn);
-                if (nf >= FL) { flush_far<TPL>(far, nf, T); nf = 0; }
-                if (nn >= FL) { flush_near<TPL>(nearE, nearH, nn, T); nn = 0; }
             }
-            // opened internal nodes -> children on the stack
+            // opened internal nodes -> children on the stack (spilling its
+            // bottom half to global memory when it would overflow)
             {
                 int nch = (act == 2) ? nb : 0;
                 int incl = warp_incl_scan(nch, lane);
                 int total = __shfl_sync(FULL, incl, 31);
-                if (sp + total > p.stack_cap) {
-                    overflow = true;
-                    break;
+                if (sp + total > WALK_SSTACK) {
+                    const int m = WALK_SSTACK / 2;
+                    if (gsp + m > p.stack_cap) {
+                        overflow = true;
+                        break;
+                    }
+                    for (int i = lane; i < m; i += 32) gstack[gsp + i] = sstack[i];
+                    __syncwarp();
+                    for (int i = lane; i < sp - m; i += 32) sstack[i] = sstack[m + i];   // sp - m <= m: no overlap
+                    __syncwarp();
+                    gsp += m;
+                    sp -= m;
                 }
                 int o = sp + incl - nch;
-                for (int c = 0; c < nch; c++) stack[o + c] = na + c;
+                for (int c = 0; c < nch; c++) sstack[o + c] = na + c;
                 sp += total;
                 __syncwarp();
             }
+            // next round's node records are loaded now; the loads complete behind
+            // this round's flushes and leaf particles
+            int next_node = -1;
+            const int next_k = pop_nodes(next_node);
+            GGNode nxt;
+            if (lane < next_k) nxt = load_node(p.nodes + next_node);
+            if (nf >= FL) { flush_far<TPL>(far, nf, T); nf = 0; }
+            if (nn >= FL) { flush_near<TPL>(nearE, nearH, nn, T); nn = 0; }
             // opened leaves -> particles, 32 at a time
             {
                 int cnt = (act == 3) ? -nb : 0;
@@ -439,6 +478,9 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
                     if (nn >= FL) { flush_near<TPL>(nearE, nearH, nn, T); nn = 0; }
                 }
             }
+            k = next_k;
+            node = next_node;
+            cur = nxt;
         }
         if (overflow) {
             if (lane == 0) atomicOr(p.err, GG_EBIT_STACK_OVERFLOW);
