@@ -38,8 +38,12 @@ WORKLOADS = {
     "galaxy": ("galaxy_hernquist_halo_3000000_exp_disk_1194304", lambda seed: ics.galaxy(seed=seed)),
     "plummer": ("plummer_65536", lambda seed: ics.plummer(65536, seed=seed)),
     "clustered": ("clustered_1000_clumps_16777216", lambda seed: ics.clustered(seed=seed)),
+    # small cases of the same models, used for ncu captures
+    "galaxy1m": ("galaxy_hernquist_halo_715000_exp_disk_285000", lambda seed: ics.galaxy(715000, 285000, seed=seed)),
+    "clustered1m": ("clustered_250_clumps_1048576", lambda seed: ics.clustered(1048576, seed=seed, n_clumps=250)),
 }
-SEEDS = {"galaxy": ics.SEED_GALAXY, "plummer": ics.SEED_PLUMMER, "clustered": ics.SEED_CLUSTERED}
+SEEDS = {"galaxy": ics.SEED_GALAXY, "plummer": ics.SEED_PLUMMER, "clustered": ics.SEED_CLUSTERED,
+         "galaxy1m": ics.SEED_GALAXY, "clustered1m": ics.SEED_CLUSTERED}
 
 
 def log(*a):
@@ -141,24 +145,25 @@ def cpu_reference_rate(ic, seconds=15.0, seed=1, tol=0.0025):
 
 
 def run_reference_arm(args):
+    """Time the reference's own CPU tree gravity (all host threads) on this
+    arm's workload: W+K steady-state steps, each a bounded sample of targets."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     name, gen = WORKLOADS[args.workload]
     ic = gen(SEEDS[args.workload])
     n = ic["pos"].shape[0]
-    # OldAcc for the relative pass: the reference's own Barnes-Hut pass is the
-    # start-up rule (accel.c:47-50); a GPU-free run takes |a| from the direct
-    # sum of a coarse model: use the Barnes-Hut pass of the C restatement.
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    vals = []
-    info = None
-    for i in range(args.warmup + args.steps):
-        r = cpu_reference_rate(ic, seconds=args.ref_seconds, seed=1000 + i, tol=args.tol)
-        if i >= args.warmup:
-            vals.append(r["value"])
-            info = r
-    v = float(np.mean(vals))
+    import ref_runner
+    if ref_runner.available():
+        rates, info = ref_runner.steps_rate(ic, steps=args.steps, warmup=args.warmup, sample_n=args.ref_sample,
+                                            tol=args.tol)
+        v = float(np.mean(rates))
+    else:
+        vals = [cpu_reference_rate(ic, seconds=args.ref_seconds, seed=1000 + i, tol=args.tol)
+                for i in range(args.warmup + args.steps)][args.warmup:]
+        v = float(np.mean([x["value"] for x in vals]))
+        info = vals[-1]
     out = {"metric": METRIC, "value": v, "unit": "particles/s", "n_gpus": args.gpus, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": 1e3 * n / v, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -179,9 +184,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="galaxy", choices=sorted(WORKLOADS))
-    ap.add_argument("--tol", type=float, default=0.0025)
+    # 0.001 keeps the galaxy's p99 force error below 2e-3 (the metric's bound)
+    ap.add_argument("--tol", type=float, default=0.001)
     ap.add_argument("--err-targets", type=int, default=65536)
     ap.add_argument("--ref-seconds", type=float, default=8.0)
+    ap.add_argument("--ref-sample", type=int, default=16384)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -344,7 +351,7 @@ def main():
     if not args.no_cpu and rank == 0 and world == 1:
         ic_cpu = dict(ic)
         ic_cpu["acc_hint"] = acc
-        cpu = cpu_reference_rate(ic_cpu, seconds=args.cpu_seconds)
+        cpu = cpu_reference_rate(ic_cpu, seconds=args.cpu_seconds, tol=args.tol)
 
     out = {
         "metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,

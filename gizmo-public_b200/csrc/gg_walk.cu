@@ -224,7 +224,10 @@ __device__ __forceinline__ int warp_incl_scan(int v, int lane)
 
 // MINB: resident blocks per SM the register allocation must allow (1..3): a
 // tuning knob trading registers (spills) against warps in flight.
-template <int TPL, int MINB>
+// F64T: opening tests in FP64 (used for one-target groups, where the tests are
+// exactly the reference's); otherwise the tests run in FP32 on FP64-formed
+// offsets from the group centre, against a bounding box rounded outwards.
+template <int TPL, int MINB, bool F64T>
 __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
 {
     extern __shared__ float4 walk_smem[];
@@ -299,6 +302,8 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
             T.z[s] = (float)(tz[s] - cg[2]);
         }
         const double hmaxd = (double)hmax, hmind = (double)hmin;
+        const float hwf[3] = {__double2float_ru(hw[0]), __double2float_ru(hw[1]), __double2float_ru(hw[2])};
+        const float aoldf = (float)aold_min, thetaf = (float)theta;
 
         // ---- traversal
         // The node stack lives in shared memory (sp entries) on top of a spill
@@ -344,6 +349,34 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
                 if (nd.mass > 0.f) {
                     if (nb == -1) {
                         act = 3;
+                    } else if (!F64T) {
+                        const float dx = (float)(nd.cx - cg[0]), dy = (float)(nd.cy - cg[1]), dz = (float)(nd.cz - cg[2]);
+                        const float ex = fmaxf(fabsf(dx) - hwf[0], 0.f), ey = fmaxf(fabsf(dy) - hwf[1], 0.f),
+                                    ez = fmaxf(fabsf(dz) - hwf[2], 0.f);
+                        const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+                        const float ms = nd.maxsoft, L = nd.len;
+                        bool open = (hmin < ms) && (r2 < ms * ms);
+                        if (!open) {
+                            if (thetaf > 0.f) {
+                                open = L * L > r2 * thetaf * thetaf;
+                            } else {
+                                const float a1 = fmaf(0.6f, L, hmax), a2 = fmaf(0.6f, L, ms);
+                                open = (r2 < a1 * a1) || (r2 < a2 * a2) || (nd.mass * L * L > r2 * r2 * aoldf);
+                                if (!open)
+                                    open = (fabsf(dx + nd.gx) < fmaf(0.6f, L, hwf[0])) &&
+                                           (fabsf(dy + nd.gy) < fmaf(0.6f, L, hwf[1])) &&
+                                           (fabsf(dz + nd.gz) < fmaf(0.6f, L, hwf[2]));
+                            }
+                        }
+                        if (open) {
+                            act = (nb > 0) ? 2 : 3;
+                        } else {
+                            act = 1;
+                            ent = make_float4(dx, dy, dz, nd.mass);
+                            hp = ms;
+                            const float hh = fmaxf(hmax, ms);
+                            isfar = (r2 >= hh * hh) && (r2 > 0.f);
+                        }
                     } else {
                         double dx = nd.cx - cg[0], dy = nd.cy - cg[1], dz = nd.cz - cg[2];
                         double ex = fmax(fabs(dx) - hw[0], 0.0), ey = fmax(fabs(dy) - hw[1], 0.0),
@@ -449,15 +482,15 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
                         int pi = a_src + (q - e_src);
                         GGPart pp = load_part(p.parts + pi);
                         if (pp.m > 0.f) {
-                            double dx = pp.x - cg[0], dy = pp.y - cg[1], dz = pp.z - cg[2];
-                            double ex = fmax(fabs(dx) - hw[0], 0.0), ey = fmax(fabs(dy) - hw[1], 0.0),
-                                   ez = fmax(fabs(dz) - hw[2], 0.0);
-                            double r2 = ex * ex + ey * ey + ez * ez;
-                            double hh = fmax(hmaxd, (double)pp.h);
-                            pe = make_float4((float)dx, (float)dy, (float)dz, pp.m);
+                            const float dx = (float)(pp.x - cg[0]), dy = (float)(pp.y - cg[1]), dz = (float)(pp.z - cg[2]);
+                            const float ex = fmaxf(fabsf(dx) - hwf[0], 0.f), ey = fmaxf(fabsf(dy) - hwf[1], 0.f),
+                                        ez = fmaxf(fabsf(dz) - hwf[2], 0.f);
+                            const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+                            const float hh = fmaxf(hmax, pp.h);
+                            pe = make_float4(dx, dy, dz, pp.m);
                             ph = pp.h;
                             use = true;
-                            pfar = (r2 >= hh * hh) && (r2 > 0.0);
+                            pfar = (r2 >= hh * hh) && (r2 > 0.f);
                         }
                     }
                     unsigned mf = __ballot_sync(FULL, use && pfar);
@@ -518,11 +551,11 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
     }
 }
 
-template <int TPL, int MINB>
+template <int TPL, int MINB, bool F64T>
 static void launch_walk_t(const WalkParams &p, int blocks, int smem, cudaStream_t st)
 {
-    cudaFuncSetAttribute(k_walk<TPL, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    k_walk<TPL, MINB><<<blocks, WALK_THREADS, smem, st>>>(p);
+    cudaFuncSetAttribute(k_walk<TPL, MINB, F64T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k_walk<TPL, MINB, F64T><<<blocks, WALK_THREADS, smem, st>>>(p);
 }
 
 // blocks_per_sm selects the register budget of the instantiation (1..3) and
@@ -532,14 +565,16 @@ void gg_launch_walk(const WalkParams &p, int tpl, int blocks_per_sm, cudaStream_
     int smem = gg_walk_smem_bytes(p.flush, tpl);
     int minb = blocks_per_sm < 1 ? 1 : (blocks_per_sm > 3 ? 3 : blocks_per_sm);
     int blocks = gg_num_sms() * blocks_per_sm;
-    if (tpl == 2) {
-        if (minb == 1) launch_walk_t<2, 1>(p, blocks, smem, st);
-        else if (minb == 2) launch_walk_t<2, 2>(p, blocks, smem, st);
-        else launch_walk_t<2, 3>(p, blocks, smem, st);
+    if (p.group_size == 1) {
+        launch_walk_t<1, 2, true>(p, blocks, smem, st);   // exact mode: the reference's tests
+    } else if (tpl == 2) {
+        if (minb == 1) launch_walk_t<2, 1, false>(p, blocks, smem, st);
+        else if (minb == 2) launch_walk_t<2, 2, false>(p, blocks, smem, st);
+        else launch_walk_t<2, 3, false>(p, blocks, smem, st);
     } else {
-        if (minb == 1) launch_walk_t<1, 1>(p, blocks, smem, st);
-        else if (minb == 2) launch_walk_t<1, 2>(p, blocks, smem, st);
-        else launch_walk_t<1, 3>(p, blocks, smem, st);
+        if (minb == 1) launch_walk_t<1, 1, false>(p, blocks, smem, st);
+        else if (minb == 2) launch_walk_t<1, 2, false>(p, blocks, smem, st);
+        else launch_walk_t<1, 3, false>(p, blocks, smem, st);
     }
     gg_note_launches(1);
 }

@@ -139,7 +139,8 @@ def types_and_eps(h):
     return t, eps1, eps2
 
 
-def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeout=3600, binary=None):
+def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeout=3600, binary=None,
+        sample_only=False):
     """Run the reference: start-up evaluation (BH pass, relative pass) and
     optional steady-state steps.  Returns dict with acc (pre-G = acc/G with
     G = 1), pot, oldacc in input order, interaction counts and timings."""
@@ -158,7 +159,7 @@ def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeou
         with open(os.path.join(d, "params"), "w") as f:
             f.write(PARAMS.format(ic=icp, out=os.path.join(d, "out"), memmb=memmb, eps1=repr(eps1), eps2=repr(eps2)))
         args = [binary or BIN, os.path.join(d, "params"), repr(tol), os.path.join(d, "res.bin")]
-        if steps:
+        if steps or sample is not None:
             args.append(str(steps))
             if sample is not None:
                 sp = os.path.join(d, "sample.bin")
@@ -167,6 +168,8 @@ def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeou
                 inv[order] = np.arange(n)
                 (inv[np.asarray(sample)] + 1).astype("<i8").tofile(sp)
                 args.append(sp)
+                if sample_only:
+                    args.append("1")
         env = dict(os.environ)
         if threads:
             env["OMP_NUM_THREADS"] = str(threads)
@@ -208,28 +211,40 @@ def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeou
             shutil.rmtree(d, ignore_errors=True)
 
 
-def rate(ic, seconds=15.0, seed=1, tol=0.0025, threads=None):
-    """Reference particles/s for one steady-state step (domain decomposition +
-    tree build + relative walk of every particle), from a bounded sample: the
-    walk is timed on a seeded random subset of active targets and scaled."""
+def steps_rate(ic, steps=3, warmup=1, sample_n=16384, seed=1, tol=0.0025, threads=None):
+    """The reference's particles/s per steady-state step, from a bounded sample.
+
+    One run of GIZMO's own code: start-up passes on a seeded random sample of
+    targets, then warmup+steps steps of domain_Decomposition (keys, sort,
+    reorder), tree build and the relative walk of the sampled targets.  A
+    step's cost for all N particles is domain + build + (walk time per sampled
+    target) x N.  Returns (per-step rates of the timed steps, info)."""
     n = ic["pos"].shape[0]
     cores = threads or os.cpu_count() or 1
-    rng = np.random.default_rng(seed)
-    ns = min(n, 2048)
-    res = None
-    for _ in range(4):
-        sample = np.sort(rng.choice(n, ns, replace=False))
-        res = run(ic, tol=tol, steps=2, sample=sample, threads=cores)
-        st = res["info"]["steps"][-1]
-        t_walk = st["t_gravity"] - st["t_build"]
-        if t_walk > 0.2 * seconds or ns >= n:
-            break
-        ns = min(n, int(ns * max(2.0, 0.3 * seconds / max(t_walk, 1e-3))))
-    per = t_walk / ns
-    step = st["t_domain"] + st["t_build"] + per * n
-    return {"value": n / step, "unit": "particles/s", "cores": cores, "kind": "reference",
-            "sample": "GIZMO's own domain_Decomposition + gravity_tree (compiled reference, FP64, OpenMP %d "
-                      "threads): full keys/sort/tree build + relative walk of %d seeded random active targets of "
-                      "%d, walk time scaled to all targets" % (cores, ns, n),
-            "t_domain_s": st["t_domain"], "t_build_s": st["t_build"], "t_walk_per_particle_us": per * 1e6,
-            "interactions_per_target": st["cost"] / ns}
+    ns = min(n, sample_n)
+    sample = np.sort(np.random.default_rng(seed).choice(n, ns, replace=False))
+    res = run(ic, tol=tol, steps=warmup + steps, sample=sample, threads=cores, sample_only=True)
+    rates, per_list = [], []
+    for st in res["info"]["steps"][warmup:]:
+        per = max(st["t_gravity"] - st["t_build"], 1e-12) / ns
+        rates.append(n / (st["t_domain"] + st["t_build"] + per * n))
+        per_list.append(per)
+    last = res["info"]["steps"][-1]
+    info = {"unit": "particles/s", "cores": cores, "kind": "reference",
+            "sample": "GIZMO's own domain_Decomposition + tree build + relative gravity walk (compiled reference, "
+                      "FP64, OpenMP %d threads) with %d seeded random active targets of %d; walk time per target "
+                      "scaled to all targets" % (cores, ns, n),
+            "t_domain_s": last["t_domain"], "t_build_s": last["t_build"],
+            "t_walk_per_particle_us": float(np.mean(per_list)) * 1e6}
+    return rates, info
+
+
+def rate(ic, seconds=15.0, seed=1, tol=0.0025, threads=None):
+    """One bounded measurement of the reference's step rate (about `seconds` of walk)."""
+    n = ic["pos"].shape[0]
+    probe, pinfo = steps_rate(ic, steps=1, warmup=0, sample_n=512, seed=seed, tol=tol, threads=threads)
+    per = pinfo["t_walk_per_particle_us"] * 1e-6
+    ns = int(min(n, max(512, seconds / max(per, 1e-9))))
+    rates, info = steps_rate(ic, steps=1, warmup=0, sample_n=ns, seed=seed + 1, tol=tol, threads=threads)
+    info["value"] = float(np.mean(rates))
+    return info
