@@ -30,6 +30,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "gizmo-public_b200"))
 
 import ics  # noqa: E402
+import multi  # noqa: E402
 
 FLOPS_PER_INTERACTION = 20   # monopole force convention (3 sub, r^2, rsqrt, m/r^3, 3 fma)
 METRIC = "tree-gravity particles/s at p99 force err<=2e-3 vs FP64 direct; serve p50/p99 ms"
@@ -205,18 +206,12 @@ def main():
     import torch
     import ggb200
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world, rank, local = multi.world()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dist = multi.init("nccl")
 
     name, gen = WORKLOADS[args.workload]
-    ic = gen(SEEDS[args.workload] + 7919 * rank)   # independent system per rank
+    ic = gen(multi.rank_seed(SEEDS[args.workload], rank))   # independent system per rank
     n = ic["pos"].shape[0]
     dev = torch.device("cuda", local)
     stream = torch.cuda.Stream(device=dev)   # every kernel and event of the bench goes on this stream
@@ -268,15 +263,8 @@ def main():
     walk_ms = sum(ev[2 * k + 1].elapsed_time(ev[2 * k + 2]) for k in range(args.steps)) / args.steps
     build_ms = (ev[0].elapsed_time(ev[1]) + sum(ev[2 * k].elapsed_time(ev[2 * k + 1])
                                                  for k in range(1, args.steps))) / args.steps
-    if dist:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-        tn = torch.tensor([float(n)], device=dev)
-        dist.all_reduce(tn)
-        n_all = float(tn.item())
-    else:
-        n_all = float(n)
+    total_ms = multi.max_over_ranks(dist, total_ms, device=dev)
+    n_all = multi.sum_over_ranks(dist, n, device=dev)
     stats = tree.last_stats()
     ms_step = total_ms / args.steps
     value = n_all / (ms_step * 1e-3)
