@@ -177,6 +177,243 @@ def run_reference_arm(args):
     return 0
 
 
+# ---------------------------------------------------------------- batched ensemble
+ENSEMBLE_NAME = "ensemble_4096_plummer_king_w6_n256_65536"
+
+
+def ensemble_error_targets(counts, per_system=16, seed=4242):
+    """Seeded sample of up to `per_system` targets in every system: (system, global index) pairs."""
+    rng = np.random.default_rng(seed)
+    off = np.concatenate([[0], np.cumsum(counts)])
+    sys_of, idx = [], []
+    for s, n in enumerate(counts):
+        k = min(per_system, int(n))
+        idx.append(off[s] + np.sort(rng.choice(int(n), k, replace=False)))
+        sys_of.append(np.full(k, s))
+    return np.concatenate(sys_of), np.concatenate(idx)
+
+
+def ensemble_direct(ic, d_pos, d_mass, d_h, counts, sys_of, idx, stream, dev):
+    """FP64 direct sum of every sampled target against the sources of its own system."""
+    import torch
+    import ggb200
+    off = np.concatenate([[0], np.cumsum(counts)])
+    acc = np.empty((idx.size, 3))
+    d_acc = torch.empty((idx.size, 3), dtype=torch.float64, device=dev)
+    d_pot = torch.empty(idx.size, dtype=torch.float64, device=dev)
+    d_tg = torch.from_numpy((idx - off[sys_of]).astype(np.int32)).to(dev)
+    starts = np.flatnonzero(np.r_[True, sys_of[1:] != sys_of[:-1]])
+    ends = np.r_[starts[1:], idx.size]
+    for a, b in zip(starts, ends):
+        s = int(sys_of[a])
+        o, n = int(off[s]), int(counts[s])
+        ggb200.direct_sum_fp64(d_pos[o:o + n], d_mass[o:o + n], d_h[o:o + n], n, d_tg[a:b], int(b - a),
+                               d_acc[a:b], d_pot[a:b], stream.cuda_stream)
+    torch.cuda.synchronize()
+    acc[:] = d_acc.cpu().numpy()
+    return acc
+
+
+def ensemble_reference_rate(ic, tol, n_sample=16, seed=77):
+    """The reference (compiled GIZMO, all host threads) run on a seeded sample
+    of whole systems of the ensemble, one process per system as it would run
+    them: particles/s = sum of N / sum of (domain + build + walk) step times."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_runner
+    if not ref_runner.available():
+        return None
+    counts = ic["counts"]
+    off = np.concatenate([[0], np.cumsum(counts)])
+    pick = np.sort(np.random.default_rng(seed).choice(counts.size, n_sample, replace=False))
+    n_tot, t_tot, cores = 0, 0.0, os.cpu_count() or 1
+    for s in pick:
+        o, n = int(off[s]), int(counts[s])
+        sub = {k: ic[k][o:o + n] for k in ("pos", "vel", "mass", "h")}
+        rates, info = ref_runner.steps_rate(sub, steps=1, warmup=0, sample_n=n, tol=tol)
+        n_tot += n
+        t_tot += n / rates[0]
+        cores = info["cores"]
+    return {"value": n_tot / t_tot, "unit": "particles/s", "cores": cores, "kind": "reference",
+            "sample": "GIZMO's own domain_Decomposition + tree build + relative walk (compiled reference, FP64, "
+                      "OpenMP %d threads), all particles active, on %d seeded whole systems of the ensemble "
+                      "(%d particles), one run per system" % (cores, n_sample, n_tot)}
+
+
+def run_ensemble(args, torch, ggb200, dist, world, rank, local):
+    """4,096 independent clusters: one batched build + walk of every system per
+    step, autotuned and replayed as one CUDA graph, against the plain form
+    (one gg_load/gg_build/gg_evaluate per system) at the same opening tolerance."""
+    ic = ics.ensemble(seed=multi.rank_seed(ics.SEED_ENSEMBLE, rank))
+    counts = np.asarray(ic["counts"], dtype=np.int64)
+    n = int(counts.sum())
+    S = counts.size
+    off = np.concatenate([[0], np.cumsum(counts)])
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    rec = ggb200.make_records(ic["pos"], ic["mass"], ic["h"])
+    d_rec = torch.from_numpy(rec.view(np.uint8)).to(dev)
+    d_acc = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    d_pot = torch.empty(n, dtype=torch.float64, device=dev)
+    tol = args.tol
+
+    tree = ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush, device=local,
+                              blocks_per_sm=args.blocks_per_sm)
+    tree.set_stream(stream.cuda_stream)
+    tree.load_device(d_rec, counts)
+    tree.build()
+    tree.evaluate_device(d_acc, d_pot, err_tol_theta=0.7)            # start-up BH pass: OldAcc
+    tree.build()
+    tree.evaluate_device(d_acc, d_pot, err_tol_force_acc=tol)         # first relative pass
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    tuned, tuned_ms = tree.autotune(err_tol_force_acc=tol) if not args.no_autotune else (None, None)
+    t_tune = time.perf_counter() - t0
+
+    # uncaptured batched step (also allocates every buffer the capture reuses)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record(stream)
+    tree.build()
+    ev[1].record(stream)
+    tree.evaluate_device(d_acc, d_pot, err_tol_force_acc=tol)
+    ev[2].record(stream)
+    torch.cuda.synchronize()
+    plain_batched_ms = ev[0].elapsed_time(ev[2])
+    build_ms, walk_ms = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+    st = tree.last_stats()
+    if st["error_word"]:
+        raise RuntimeError("device error word %d" % st["error_word"])
+    inter = st["interactions"]
+
+    tree.capture_step(d_acc, d_pot, err_tol_force_acc=tol)
+    for _ in range(args.warmup):
+        tree.launch_step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = ggb200.kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        tree.launch_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = ggb200.kernel_launches() - launches0
+    clk = clocks.stop()
+    total_ms = multi.max_over_ranks(dist, e0.elapsed_time(e1), device=dev)
+    n_all = multi.sum_over_ranks(dist, n, device=dev)
+    ms_step = total_ms / args.steps
+    value = n_all / (ms_step * 1e-3)
+    st = tree.last_stats()
+    if st["error_word"]:
+        raise RuntimeError("device error word %d after graph replays" % st["error_word"])
+    acc_b = d_acc.cpu().numpy()
+    old = torch.linalg.norm(d_acc, dim=1).contiguous()
+
+    # plain form: one load + build + evaluate per system, same tolerance and OldAcc
+    d_acc_p = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    d_pot_p = torch.empty(n, dtype=torch.float64, device=dev)
+    plain = ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush, device=local,
+                               blocks_per_sm=args.blocks_per_sm)
+    plain.set_stream(stream.cuda_stream)
+
+    def plain_pass():
+        for s in range(S):
+            o, m = int(off[s]), int(counts[s])
+            plain.load_device(d_rec[o * 32:(o + m) * 32], [m])
+            plain.build()
+            plain.evaluate_device(d_acc_p[o:o + m], d_pot_p[o:o + m], d_old_acc=old[o:o + m],
+                                  err_tol_force_acc=tol)
+    plain_pass()
+    torch.cuda.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    plain_pass()
+    p1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = p0.elapsed_time(p1)
+    plain.close()
+    acc_p = d_acc_p.cpu().numpy()
+
+    # force errors: FP64 direct sum inside each system, 16 sampled targets per system
+    d_pos = torch.from_numpy(ic["pos"]).to(dev)
+    d_mass = torch.from_numpy(ic["mass"]).to(dev)
+    d_h = torch.from_numpy(ic["h"]).to(dev)
+    sys_of, idx = ensemble_error_targets(counts)
+    acc_dir = ensemble_direct(ic, d_pos, d_mass, d_h, counts, sys_of, idx, stream, dev)
+    del d_pos, d_mass, d_h
+    b50, b99, eb = ics.error_stats(acc_b[idx], acc_dir)
+    q50, q99, _ = ics.error_stats(acc_p[idx], acc_dir)
+    worst_sys = float(max(np.percentile(eb[sys_of == s], 99) for s in np.unique(sys_of)[:64]))
+
+    peak32 = ggb200.fp32_peak_tflops(stream.cuda_stream)
+    walk_tflops = inter * FLOPS_PER_INTERACTION / (walk_ms * 1e-3) / 1e12
+
+    e2e = None
+    if not args.no_e2e and rank == 0:
+        with ggb200.GravityTree(leaf_size=tuned["leaf_size"] if tuned else args.leaf,
+                                group_size=tuned["group_size"] if tuned else args.group,
+                                flush=tuned["flush"] if tuned else args.flush, device=local,
+                                blocks_per_sm=tuned["blocks_per_sm"] if tuned else args.blocks_per_sm) as te:
+            old_h = np.linalg.norm(acc_b, axis=1)
+
+            def e2e_step():
+                te.load(ic["pos"], ic["mass"], ic["h"], counts=counts)
+                te.build()
+                return te.evaluate(old_acc=old_h, err_tol_force_acc=tol)
+            e2e_step()
+            t0 = time.perf_counter()
+            ke = 3
+            for _ in range(ke):
+                e2e_step()
+            dt = (time.perf_counter() - t0) / ke
+        e2e = {"value": n / dt, "unit": "particles/s", "h2d_bytes_per_step": int(n * (32 + 8)),
+               "d2h_bytes_per_step": int(n * (24 + 8)), "ms_per_step": dt * 1e3,
+               "path": "gg_load_particles (host FP64 arrays, 4096 systems) + gg_build + gg_evaluate (host outputs)"}
+
+    cpu = None
+    if not args.no_cpu and rank == 0 and world == 1:
+        cpu = ensemble_reference_rate(ic, tol)
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": ENSEMBLE_NAME, "n_systems": S, "n": n, "n_total": int(n_all),
+                   "err_tol_force_acc": tol, "tuned": tuned, "autotune_walk_ms": tuned_ms, "autotune_s": t_tune,
+                   "step": "one CUDA graph: extent+keys+sort+permute+tree+moments+relative walk of every system",
+                   "l2": "inputs larger than L2 (1.5 GB of records)",
+                   "parallelism": "independent ensemble per GPU" if world > 1 else "1 GPU"},
+        "batched_vs_plain": {"graph_ms": ms_step, "batched_uncaptured_ms": plain_batched_ms, "plain_ms": plain_ms,
+                             "speedup": plain_ms / ms_step,
+                             "plain_form": "per system: gg_load_particles_device + gg_build + gg_evaluate_device, "
+                                           "default configuration, same OldAcc and tolerance"},
+        "force_error": {"p50": b50, "p99": b99, "plain_p50": q50, "plain_p99": q99, "targets": int(idx.size),
+                        "worst_system_p99_first64": worst_sys,
+                        "vs": "FP64 direct sum inside each system (GPU, same pair rule)"},
+        "interactions_per_step": inter, "interactions_per_s": inter / (ms_step * 1e-3),
+        "interactions_per_particle": inter / n,
+        "stage_ms": {"build": build_ms, "walk": walk_ms},
+        "roofline": {"bound": "fp32", "kernel": "k_walk", "achieved": walk_tflops, "peak": peak32,
+                     "unit": "TFLOP/s", "frac": walk_tflops / peak32, "traffic": None,
+                     "flops_per_interaction": FLOPS_PER_INTERACTION,
+                     "peak_source": "measured FP32 FMA probe (gg_fp32_peak_probe) on this GPU"},
+        "clocks": clk, "gpu_launches": int(launches), "e2e": e2e, "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    tree.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
 # ---------------------------------------------------------------- GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -184,7 +421,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="galaxy", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="galaxy", choices=sorted(WORKLOADS) + ["ensemble"])
     # 0.001 keeps the galaxy's p99 force error below 2e-3 (the metric's bound)
     ap.add_argument("--tol", type=float, default=0.001)
     ap.add_argument("--err-targets", type=int, default=65536)
@@ -197,6 +434,7 @@ def main():
     ap.add_argument("--group", type=int, default=32)
     ap.add_argument("--flush", type=int, default=64)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -209,6 +447,8 @@ def main():
     world, rank, local = multi.world()
     torch.cuda.set_device(local)
     dist = multi.init("nccl")
+    if args.workload == "ensemble":
+        return run_ensemble(args, torch, ggb200, dist, world, rank, local)
 
     name, gen = WORKLOADS[args.workload]
     ic = gen(multi.rank_seed(SEEDS[args.workload], rank))   # independent system per rank

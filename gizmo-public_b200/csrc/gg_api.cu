@@ -94,6 +94,7 @@ struct gg_ctx {
     DevBuf<GGNode> nodes;
     // walk
     DevBuf<double> oldacc;
+    DevBuf<double> oldacc_save;           // autotuner: every trial starts from the same OldAcc
     bool oldacc_valid = false;
     DevBuf<GGGroup> groups;
     DevBuf<int> ngroups, gscan, toff, flag, flagscan, tlist, tout, scan_scratch, active_d;
@@ -109,6 +110,10 @@ struct gg_ctx {
     size_t h_stage_cap = 0;
     // timing
     cudaEvent_t ev[8];
+    // a captured step (build + walk) replayed as one CUDA graph
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_launches = 0;               // kernels inside the captured step
     bool have_events = false;
     gg_stats last;
 };
@@ -198,6 +203,8 @@ extern "C" gg_status gg_destroy(gg_ctx *c)
     c->active_d.release(); c->counters.release(); c->inter.release(); c->stack.release(); c->err.release();
     c->acc_d.release(); c->pot_d.release(); c->nint_d.release();
     if (c->h_stage) cudaFreeHost(c->h_stage);
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
     if (c->have_events)
         for (int i = 0; i < 8; i++) cudaEventDestroy(c->ev[i]);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -628,4 +635,129 @@ extern "C" gg_status gg_direct_sum_fp64(int64_t n_src, const double *d_pos, cons
     gg_launch_direct(n_src, d_pos, d_mass, d_h, n_tgt, d_targets, d_acc, d_pot, (cudaStream_t)stream);
     GG_CUDA_TRY(cudaGetLastError());
     return GG_OK;
+}
+
+// ---------------------------------------------------------------- graphs and autotuning
+// One step of a resident batch (keys, sort, tree, moments, walk of every
+// target of every system) captured once and replayed as a single CUDA graph.
+// The capture reuses the context's buffers, so the step must have run once
+// uncaptured with the same systems (every buffer is then already allocated
+// and nothing inside the capture allocates or synchronises).
+extern "C" gg_status gg_graph_capture_step(gg_ctx *c, double tol, double theta, double *d_acc, double *d_pot)
+{
+    if (!c || !d_acc || tol < 0 || theta < 0) return GG_ERR_INVALID;
+    if (!c->built) return GG_ERR_NOT_BUILT;
+    if (!c->stream) return GG_ERR_INVALID;   // the legacy default stream cannot be captured
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+    if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
+    // grow every buffer the walk may need before capturing
+    if ((st = walk_setup(c))) return st;
+    const int timing = c->cfg.timing;
+    c->cfg.timing = 0;
+    long long before = gg_kernel_launches();
+    GG_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    st = gg_build(c, nullptr);
+    if (!st) st = run_walk(c, nullptr, 0, nullptr, tol, theta, d_acc, d_pot, nullptr);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    c->cfg.timing = timing;
+    if (st) { if (g) cudaGraphDestroy(g); return st; }
+    if (e != cudaSuccess) return gg_cuda_fail(e);
+    c->graph_launches = (int)(gg_kernel_launches() - before);
+    c->graph = g;
+    e = cudaGraphInstantiate(&c->graph_exec, g, 0);
+    if (e != cudaSuccess) { cudaGraphDestroy(g); c->graph = nullptr; c->graph_exec = nullptr; return gg_cuda_fail(e); }
+    return GG_OK;
+}
+
+extern "C" gg_status gg_graph_launch(gg_ctx *c)
+{
+    if (!c) return GG_ERR_INVALID;
+    if (!c->graph_exec) return GG_ERR_NOT_BUILT;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    GG_CUDA_TRY(cudaGraphLaunch(c->graph_exec, c->stream));
+    gg_note_launches(c->graph_launches);
+    return GG_OK;
+}
+
+// Timed search over the walk's tunables on the resident systems: leaf size
+// (rebuilds the tree), group size (targets per warp), blocks per SM (stack
+// depth per warp follows from it) and the list-flush threshold.  Every trial
+// walks from the same OldAcc, so trials see the same opening decisions for a
+// given tree; the fastest configuration is kept and the tree rebuilt with it.
+extern "C" gg_status gg_autotune(gg_ctx *c, double tol, double theta, gg_config *chosen, double *best_ms)
+{
+    if (!c || tol < 0 || theta < 0) return GG_ERR_INVALID;
+    if (!c->built) return GG_ERR_NOT_BUILT;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    cudaStream_t s = c->stream;
+    const long long N = c->N;
+    if ((st = c->acc_d.ensure(N * 3 + 3))) return st;
+    const bool had_old = c->oldacc_valid;
+    if (had_old && ((st = c->oldacc_save.ensure(N + 1)))) return st;
+    if (had_old)
+        GG_CUDA_TRY(cudaMemcpyAsync(c->oldacc_save.p, c->oldacc.p, N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    cudaEvent_t e0, e1;
+    GG_CUDA_TRY(cudaEventCreate(&e0));
+    GG_CUDA_TRY(cudaEventCreate(&e1));
+    const gg_config base = c->cfg;
+    const int base_blocks = c->walk_blocks;
+    static const int leafs[] = {8, 16}, groups[] = {32, 64}, bpss[] = {2, 3}, flushes[] = {64, 96};
+    float best = 1e30f;
+    gg_config best_cfg = base;
+    int best_blocks = base_blocks;
+    st = GG_OK;
+    for (int li = 0; li < 2 && !st; li++) {
+        c->cfg.leaf_size = leafs[li];
+        if ((st = gg_build(c, nullptr))) break;
+        for (int gi = 0; gi < 2 && !st; gi++)
+            for (int bi = 0; bi < 2 && !st; bi++)
+                for (int fi = 0; fi < 2 && !st; fi++) {
+                    c->cfg.group_size = groups[gi];
+                    c->cfg.flush_threshold = flushes[fi];
+                    c->walk_blocks = bpss[bi];
+                    float ms_min = 1e30f;
+                    for (int rep = 0; rep < 2 && !st; rep++) {
+                        if (had_old) {
+                            cudaError_t ce = cudaMemcpyAsync(c->oldacc.p, c->oldacc_save.p, N * sizeof(double),
+                                                             cudaMemcpyDeviceToDevice, s);
+                            if (ce != cudaSuccess) { st = gg_cuda_fail(ce); break; }
+                        }
+                        c->oldacc_valid = had_old;
+                        cudaEventRecord(e0, s);
+                        st = run_walk(c, nullptr, 0, nullptr, tol, theta, c->acc_d.p, nullptr, nullptr);
+                        cudaEventRecord(e1, s);
+                        if (st) break;
+                        st = collect_stats(c, nullptr);
+                        float ms = 0;
+                        cudaEventElapsedTime(&ms, e0, e1);
+                        if (ms < ms_min) ms_min = ms;
+                    }
+                    if (!st && ms_min < best) {
+                        best = ms_min;
+                        best_cfg = c->cfg;
+                        best_blocks = c->walk_blocks;
+                    }
+                }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // keep the winner (or restore the original configuration after a failure)
+    c->cfg = st ? base : best_cfg;
+    c->walk_blocks = st ? base_blocks : best_blocks;
+    c->cfg.walk_blocks_per_sm = c->walk_blocks;
+    gg_status st2 = gg_build(c, nullptr);
+    if (had_old) {
+        cudaError_t ce = cudaMemcpyAsync(c->oldacc.p, c->oldacc_save.p, N * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        if (ce != cudaSuccess && !st2) st2 = gg_cuda_fail(ce);
+    }
+    c->oldacc_valid = had_old;
+    if (!st) st = st2;
+    if (!st && chosen) *chosen = c->cfg;
+    if (!st && best_ms) *best_ms = best;
+    return st;
 }

@@ -112,6 +112,9 @@ def load_library():
             "gg_fp32_peak_probe": (i32, [ctypes.POINTER(dbl), P]),
             "gg_radix_sort_pairs_noalloc": (i32, [i64, P, P, i32, P]),
             "gg_kernel_launches": (i64, []),
+            "gg_graph_capture_step": (i32, [P, dbl, dbl, P, P]),
+            "gg_graph_launch": (i32, [P]),
+            "gg_autotune": (i32, [P, dbl, dbl, ctypes.POINTER(Config), ctypes.POINTER(dbl)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -248,6 +251,26 @@ class GravityTree:
         st = Stats()
         _check(self._lib.gg_last_stats(self._h, ctypes.byref(st)), "gg_last_stats")
         return st.as_dict()
+
+    def capture_step(self, d_acc, d_pot=None, err_tol_force_acc=0.0025, err_tol_theta=0.0):
+        """Capture build + walk of every resident system as one CUDA graph (the
+        context needs its own stream, see set_stream, and one uncaptured step)."""
+        _check(self._lib.gg_graph_capture_step(self._h, err_tol_force_acc, err_tol_theta, _ptr(d_acc), _ptr(d_pot)),
+               "gg_graph_capture_step")
+
+    def launch_step(self):
+        """Replay the captured step on the context's stream (asynchronous)."""
+        _check(self._lib.gg_graph_launch(self._h), "gg_graph_launch")
+
+    def autotune(self, err_tol_force_acc=0.0025, err_tol_theta=0.0):
+        """Pick leaf size, group size, blocks per SM and flush threshold by
+        timing the walk of the resident systems; returns (config dict, ms)."""
+        cfg = Config()
+        ms = ctypes.c_double()
+        _check(self._lib.gg_autotune(self._h, err_tol_force_acc, err_tol_theta, ctypes.byref(cfg), ctypes.byref(ms)),
+               "gg_autotune")
+        return dict(leaf_size=cfg.leaf_size, group_size=cfg.group_size, flush=cfg.flush_threshold,
+                    blocks_per_sm=cfg.walk_blocks_per_sm), ms.value
 
 
 def gravity_tree(pos, mass, h, G=1.0, err_tol_force_acc=0.0025, err_tol_theta=0.7, active=None, tree=None,

@@ -132,6 +132,28 @@ gg_status gg_evaluate_device(gg_ctx *ctx, const int32_t *d_active, int64_t n_act
 /* interaction count and error word of the last evaluation (synchronises) */
 gg_status gg_last_stats(gg_ctx *ctx, gg_stats *stats);
 
+/* ---- batched steps ------------------------------------------------------
+ * No counterpart in the reference, which walks one system per process.  A
+ * step of every resident system -- gg_build(ctx, NULL) then
+ * gg_evaluate_device of all targets with d_acc_out / d_pot_out -- captured
+ * once as a CUDA graph and replayed by gg_graph_launch on the context's
+ * stream (set one with gg_set_stream first: the legacy default stream cannot
+ * be captured).  Run one uncaptured build + evaluation with the same systems
+ * before capturing, so that every buffer is allocated.  A replay re-reads the
+ * particles last loaded into the same buffers and keeps the relative
+ * criterion's OldAcc on the device between replays.  Loading a system set of
+ * a different total size invalidates the graph; capture again. */
+gg_status gg_graph_capture_step(gg_ctx *ctx, double err_tol_force_acc, double err_tol_theta, double *d_acc_out,
+                                double *d_pot_out);
+gg_status gg_graph_launch(gg_ctx *ctx);
+/* Times the walk of the resident systems over leaf size {8,16}, group size
+ * {32,64}, blocks per SM {2,3} and flush threshold {64,96}, each trial from the
+ * same OldAcc, keeps the fastest in the context (rebuilding the tree with its
+ * leaf size) and returns it in *chosen and its walk time in *best_ms
+ * (nullable).  Synchronises. */
+gg_status gg_autotune(gg_ctx *ctx, double err_tol_force_acc, double err_tol_theta, gg_config *chosen,
+                      double *best_ms);
+
 /* ---- kernel-level entry points (device pointers, cudaStream_t or NULL) ---- */
 /* domain_double_to_int (domain.c:2504-2513) + peano_hilbert_key (peano.c:303-319)
  * at 21 bits per dimension: equals the reference's 42-bit key shifted right by 63 */

@@ -1,0 +1,114 @@
+"""Batched ensembles: CUDA-graph replay of a whole step and the autotuner.
+
+A graph replay must compute exactly what the same uncaptured step computes
+(same tree, same OldAcc on the device), and the configuration the autotuner
+picks must keep the force error of every system within the bound the default
+configuration meets, checked against the FP64 direct sum inside each system.
+"""
+import numpy as np
+import pytest
+
+import ggb200
+import ics
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _ensemble(S=24, nmax=6000, seed=9):
+    return ics.ensemble(n_systems=S, nmin=256, nmax=nmax, seed=seed)
+
+
+def _setup(torch, ic, stream, **kw):
+    n = ic["pos"].shape[0]
+    rec = ggb200.make_records(ic["pos"], ic["mass"], ic["h"])
+    d_rec = torch.from_numpy(rec.view(np.uint8)).cuda()
+    t = ggb200.GravityTree(**kw)
+    t.set_stream(stream.cuda_stream)
+    t.load_device(d_rec, ic["counts"])
+    acc = torch.empty((n, 3), dtype=torch.float64, device="cuda")
+    pot = torch.empty(n, dtype=torch.float64, device="cuda")
+    t.build()
+    t.evaluate_device(acc, pot, err_tol_theta=0.7)
+    t.build()
+    t.evaluate_device(acc, pot, err_tol_force_acc=0.001)
+    return t, d_rec, acc, pot
+
+
+def test_graph_replay_equals_uncaptured_steps():
+    import torch
+    ic = _ensemble()
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        ta, _, acc_a, pot_a = _setup(torch, ic, stream)
+        tb, _, acc_b, pot_b = _setup(torch, ic, stream)
+        ref = []
+        for _ in range(3):                       # uncaptured steps, OldAcc carried on the device
+            ta.build()
+            ta.evaluate_device(acc_a, pot_a, err_tol_force_acc=0.001)
+            ref.append((acc_a.clone(), pot_a.clone()))
+        # capture needs every buffer allocated: one uncaptured step first, then restart
+        # both contexts from the same state by rerunning the start-up passes
+        tb.build()
+        tb.evaluate_device(acc_b, pot_b, err_tol_force_acc=0.001)
+        tb.build()
+        tb.evaluate_device(acc_b, pot_b, err_tol_theta=0.7)
+        tb.build()
+        tb.evaluate_device(acc_b, pot_b, err_tol_force_acc=0.001)
+        tb.capture_step(acc_b, pot_b, err_tol_force_acc=0.001)
+        for k in range(3):
+            launches0 = ggb200.kernel_launches()
+            tb.launch_step()
+            assert ggb200.kernel_launches() > launches0
+            torch.cuda.synchronize()
+            assert torch.equal(acc_b, ref[k][0]) and torch.equal(pot_b, ref[k][1]), "replay %d differs" % k
+        sa, sb = ta.last_stats(), tb.last_stats()
+        assert sa["interactions"] == sb["interactions"] and sb["error_word"] == 0
+        ta.close()
+        tb.close()
+
+
+def test_capture_and_launch_reject_bad_calls():
+    t = ggb200.GravityTree()
+    with pytest.raises(ggb200.GravityError):
+        t.launch_step()                          # nothing captured
+    ic = ics.plummer(2000, seed=3)
+    t.load(ic["pos"], ic["mass"], ic["h"])
+    with pytest.raises(ggb200.GravityError):
+        t.capture_step(None)                     # no output buffer
+    t.close()
+
+
+def _per_system_p99(ic, acc, per=24, seed=5):
+    rng = np.random.default_rng(seed)
+    off = np.concatenate([[0], np.cumsum(ic["counts"])])
+    worst = 0.0
+    for s, n in enumerate(ic["counts"]):
+        o, n = int(off[s]), int(n)
+        tg = np.sort(rng.choice(n, min(per, n), replace=False)).astype(np.int32)
+        a_dir = oracle.direct_sum(ic["pos"][o:o + n], ic["mass"][o:o + n], ic["h"][o:o + n], targets=tg)[0]
+        _, p99, _ = ics.error_stats(acc[o + tg], a_dir)
+        worst = max(worst, p99)
+    return worst
+
+
+def test_autotune_keeps_the_force_error_and_returns_a_valid_config():
+    import torch
+    ic = _ensemble(S=16, nmax=4000, seed=11)
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        t, _, acc, pot = _setup(torch, ic, stream)
+        t.build()
+        t.evaluate_device(acc, pot, err_tol_force_acc=0.001)
+        torch.cuda.synchronize()
+        base = _per_system_p99(ic, acc.cpu().numpy())
+        cfg, ms = t.autotune(err_tol_force_acc=0.001)
+        assert cfg["leaf_size"] in (8, 16) and cfg["group_size"] in (32, 64)
+        assert cfg["flush"] in (64, 96) and cfg["blocks_per_sm"] in (2, 3) and ms > 0
+        t.build()
+        t.evaluate_device(acc, pot, err_tol_force_acc=0.001)
+        torch.cuda.synchronize()
+        assert t.last_stats()["error_word"] == 0
+        tuned = _per_system_p99(ic, acc.cpu().numpy())
+        assert tuned < 2e-3 and tuned <= 1.5 * base + 1e-4
+        t.close()
