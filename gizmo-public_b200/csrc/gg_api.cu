@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <vector>
 
 #include "gg_internal.cuh"
@@ -94,6 +95,17 @@ struct gg_ctx {
     DevBuf<GGNode> nodes;
     // walk
     DevBuf<double> oldacc;
+    // drift of the resident tree (force_drift_node): velocities in load order,
+    // node kinematics {vs, vmax} of the current build, per-system steps
+    DevBuf<double> vel;
+    bool have_vel = false;
+    DevBuf<double4> kin;
+    DevBuf<int> kin_counter;
+    bool kin_valid = false;
+    bool kin_any = false;                  // kinematics computed at least once for this build
+    DevBuf<double> dts;
+    double *h_vstage = nullptr;
+    size_t h_vstage_cap = 0;
     DevBuf<double> oldacc_save;           // autotuner: every trial starts from the same OldAcc
     bool oldacc_valid = false;
     DevBuf<GGGroup> groups;
@@ -202,6 +214,8 @@ extern "C" gg_status gg_destroy(gg_ctx *c)
     c->flag.release(); c->flagscan.release(); c->tlist.release(); c->tout.release(); c->scan_scratch.release();
     c->active_d.release(); c->counters.release(); c->inter.release(); c->stack.release(); c->err.release();
     c->acc_d.release(); c->pot_d.release(); c->nint_d.release();
+    c->vel.release(); c->kin.release(); c->kin_counter.release(); c->dts.release(); c->oldacc_save.release();
+    if (c->h_vstage) cudaFreeHost(c->h_vstage);
     if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
@@ -244,6 +258,8 @@ static gg_status set_systems(gg_ctx *c, int S, const int64_t *counts)
     c->h_poff = poff;
     c->built = false;
     c->oldacc_valid = false;
+    c->have_vel = false;
+    c->kin_valid = false;
     gg_status st;
     if ((st = c->poff.ensure(S + 1))) return st;
     GG_CUDA_TRY(cudaMemcpyAsync(c->poff.p, poff.data(), (S + 1) * sizeof(int), cudaMemcpyHostToDevice, c->stream));
@@ -387,6 +403,8 @@ extern "C" gg_status gg_build(gg_ctx *c, const gg_domain *domains)
     if (timing) cudaEventRecord(c->ev[3], s);
     GG_CUDA_TRY(cudaGetLastError());
     c->built = true;
+    c->kin_valid = false;
+    c->kin_any = false;
     return GG_OK;
 }
 
@@ -760,4 +778,90 @@ extern "C" gg_status gg_autotune(gg_ctx *c, double tol, double theta, gg_config 
     if (!st && chosen) *chosen = c->cfg;
     if (!st && best_ms) *best_ms = best;
     return st;
+}
+
+// ---------------------------------------------------------------- drift
+extern "C" gg_status gg_load_velocities(gg_ctx *c, const double *vel, int64_t vel_stride)
+{
+    if (!c || !vel || c->S < 1) return GG_ERR_INVALID;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    if (vel_stride <= 0) vel_stride = 3 * sizeof(double);
+    const long long N = c->N;
+    if ((st = c->vel.ensure((size_t)3 * N + 3))) return st;
+    if ((size_t)N > c->h_vstage_cap) {
+        if (c->h_vstage) cudaFreeHost(c->h_vstage);
+        c->h_vstage = nullptr;
+        c->h_vstage_cap = 0;
+        GG_CUDA_TRY(cudaMallocHost((void **)&c->h_vstage, (size_t)(N ? N : 1) * 3 * sizeof(double)));
+        c->h_vstage_cap = (size_t)(N ? N : 1);
+    }
+    GG_CUDA_TRY(cudaStreamSynchronize(c->stream));   // staging buffer may still feed a previous copy
+    const char *vb = (const char *)vel;
+    double *dst = c->h_vstage;
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < N; i++) {
+        const double *v = (const double *)(vb + i * vel_stride);
+        dst[3 * i] = v[0]; dst[3 * i + 1] = v[1]; dst[3 * i + 2] = v[2];
+    }
+    if (N) GG_CUDA_TRY(cudaMemcpyAsync(c->vel.p, dst, (size_t)N * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    c->have_vel = true;
+    c->kin_valid = false;
+    return GG_OK;
+}
+
+extern "C" gg_status gg_load_velocities_device(gg_ctx *c, const double *d_vel)
+{
+    if (!c || !d_vel || c->S < 1) return GG_ERR_INVALID;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    if ((st = c->vel.ensure((size_t)3 * c->N + 3))) return st;
+    if (c->N)
+        GG_CUDA_TRY(cudaMemcpyAsync(c->vel.p, d_vel, (size_t)c->N * 3 * sizeof(double), cudaMemcpyDeviceToDevice,
+                                    c->stream));
+    c->have_vel = true;
+    c->kin_valid = false;
+    return GG_OK;
+}
+
+// dt_host: one step per system, or NULL for `dt_all` everywhere (no host copy,
+// so the call stays asynchronous)
+static gg_status drift_common(gg_ctx *c, const double *dt_host, double dt_all)
+{
+    if (!c) return GG_ERR_INVALID;
+    if (!c->built) return GG_ERR_NOT_BUILT;
+    if (!c->have_vel) return GG_ERR_INVALID;
+    if (!std::isfinite(dt_all)) return GG_ERR_INVALID;
+    for (int s = 0; dt_host && s < c->S; s++)
+        if (!std::isfinite(dt_host[s])) return GG_ERR_INVALID;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    if ((st = c->kin.ensure(c->ncap)) || (st = c->kin_counter.ensure(c->ncap)) || (st = c->dts.ensure(c->S)))
+        return st;
+    cudaStream_t s = c->stream;
+    if (!c->kin_valid) {
+        GG_CUDA_TRY(cudaMemsetAsync(c->kin_counter.p, 0, (size_t)c->ncap * sizeof(int), s));
+        gg_launch_node_kinematics(c->part.p, c->perm.p, c->vel.p, tree_buf(c), c->kin_counter.p, c->kin.p, (int)c->N,
+                                  c->ncap, c->kin_any ? 1 : 0, s);
+        c->kin_valid = true;
+        c->kin_any = true;
+    }
+    // pageable source: the copy has taken the values when it returns
+    if (dt_host)
+        GG_CUDA_TRY(cudaMemcpyAsync(c->dts.p, dt_host, (size_t)c->S * sizeof(double), cudaMemcpyHostToDevice, s));
+    gg_launch_drift(c->in_rec.p, c->part.p, c->perm.p, c->vel.p, c->poff.p, c->S, dt_host ? c->dts.p : nullptr,
+                    dt_all, c->nodes.p, c->kin.p, c->t_sys.p, c->t_nnodes.p, (int)c->N, c->ncap, s);
+    GG_CUDA_TRY(cudaGetLastError());
+    return GG_OK;
+}
+
+extern "C" gg_status gg_drift(gg_ctx *c, double dt)
+{
+    return drift_common(c, nullptr, dt);
+}
+
+extern "C" gg_status gg_drift_systems(gg_ctx *c, const double *dt)
+{
+    if (!c || !dt) return GG_ERR_INVALID;
+    return drift_common(c, dt, 0.0);
 }

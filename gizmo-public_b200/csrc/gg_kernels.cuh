@@ -73,3 +73,10 @@ gg_status gg_order_targets_by_softening(int nt, const int *tlist_in, const int *
 
 void gg_launch_direct(long long n_src, const double *pos, const double *mass, const double *h, long long n_tgt,
                       const int *targets, double *acc, double *pot, cudaStream_t st);
+
+// drift of a resident tree (gg_drift.cu)
+void gg_launch_node_kinematics(const GGPart *parts, const unsigned *perm, const double *vel, TreeBuf tb, int *counter,
+                               double4 *kin, int n, int ncap, int keep_max, cudaStream_t st);
+void gg_launch_drift(GGPart *in_rec, GGPart *parts, const unsigned *perm, const double *vel, const int *poff, int S,
+                     const double *dts, double dt_all, GGNode *nodes, const double4 *kin, const int *node_sys, const int *nnodes,
+                     int n, int ncap, cudaStream_t st);

@@ -112,6 +112,10 @@ def load_library():
             "gg_fp32_peak_probe": (i32, [ctypes.POINTER(dbl), P]),
             "gg_radix_sort_pairs_noalloc": (i32, [i64, P, P, i32, P]),
             "gg_kernel_launches": (i64, []),
+            "gg_load_velocities": (i32, [P, P, i64]),
+            "gg_load_velocities_device": (i32, [P, P]),
+            "gg_drift": (i32, [P, dbl]),
+            "gg_drift_systems": (i32, [P, P]),
             "gg_graph_capture_step": (i32, [P, dbl, dbl, P, P]),
             "gg_graph_launch": (i32, [P]),
             "gg_autotune": (i32, [P, dbl, dbl, ctypes.POINTER(Config), ctypes.POINTER(dbl)]),
@@ -251,6 +255,23 @@ class GravityTree:
         st = Stats()
         _check(self._lib.gg_last_stats(self._h, ctypes.byref(st)), "gg_last_stats")
         return st.as_dict()
+
+    def load_velocities(self, vel):
+        """Per-particle velocities (N,3) in load order: host array or device tensor."""
+        if isinstance(vel, np.ndarray):
+            v = np.ascontiguousarray(vel, dtype=np.float64)
+            _check(self._lib.gg_load_velocities(self._h, v.ctypes.data, 24), "gg_load_velocities")
+        else:
+            _check(self._lib.gg_load_velocities_device(self._h, _ptr(vel)), "gg_load_velocities_device")
+
+    def drift(self, dt):
+        """Move particles and nodes of the resident tree by dt (a number), or by
+        one dt per system (a sequence), without a rebuild."""
+        if np.ndim(dt) == 0:
+            _check(self._lib.gg_drift(self._h, float(dt)), "gg_drift")
+        else:
+            d = np.ascontiguousarray(dt, dtype=np.float64)
+            _check(self._lib.gg_drift_systems(self._h, d.ctypes.data), "gg_drift_systems")
 
     def capture_step(self, d_acc, d_pot=None, err_tol_force_acc=0.0025, err_tol_theta=0.0):
         """Capture build + walk of every resident system as one CUDA graph (the

@@ -14,7 +14,11 @@
  * nothing is copied on the host except the per-particle kernel radii
  * (ForceSoftening_KernelRadius, proto.h:134-155) and the active index list
  * (the FirstActiveParticle / NextActiveParticle chain, run.c:473-496).
- * Single MPI rank per GPU.
+ * Between rebuilds the reference's walk drifts particles and nodes to the
+ * current time itself (drift_particle and force_drift_node, called lazily at
+ * forcetree.c:1841 and :2051-2057); here the resident device tree is drifted
+ * instead, with the current P[].Vel, over the interval since the previous
+ * walk.  Single MPI rank per GPU.
  */
 #include <math.h>
 #include <stdio.h>
@@ -29,6 +33,7 @@ static gg_ctx *gg_tree_ctx = NULL;
 static double *gg_soft = NULL, *gg_oldacc = NULL, *gg_acc = NULL, *gg_pot = NULL;
 static int32_t *gg_active = NULL;
 static long gg_cap = 0;
+static integertime gg_tree_ti = 0;   /* integer time the device tree's positions belong to */
 
 static void gg_fail(const char *what, gg_status st)
 {
@@ -72,6 +77,24 @@ void gravtree_b200_build(void)
                            (int64_t)sizeof(struct particle_data), gg_soft, (int64_t)sizeof(double));
     if (st) gg_fail("gg_load_particles", st);
     if ((st = gg_build(gg_tree_ctx, NULL))) gg_fail("gg_build", st);
+    gg_tree_ti = All.Ti_Current;
+}
+
+/* Bring the resident tree to All.Ti_Current without a rebuild: particles move
+ * by Vel*dt (predict.c:97-137), nodes by force_drift_node
+ * (forcetree_update.c:265-338).  Velocities do not change between two walks
+ * (kicks come after the force computation), so one drift per walk interval
+ * with the current velocities follows the reference's drift. */
+static void gravtree_b200_drift(void)
+{
+    gg_status st;
+    if (All.Ti_Current == gg_tree_ti) return;
+    double dt = All.ComovingIntegrationOn ? get_drift_factor(gg_tree_ti, All.Ti_Current)
+                                          : (All.Ti_Current - gg_tree_ti) * All.Timebase_interval;
+    st = gg_load_velocities(gg_tree_ctx, &P[0].Vel[0], (int64_t)sizeof(struct particle_data));
+    if (st) gg_fail("gg_load_velocities", st);
+    if ((st = gg_drift(gg_tree_ctx, dt))) gg_fail("gg_drift", st);
+    gg_tree_ti = All.Ti_Current;
 }
 
 /* Local walk: replaces the force_treeevaluate loop over the active particles
@@ -84,6 +107,7 @@ double gravtree_b200_walk(void)
     int i;
     long n = 0;
     gg_reserve(NumPart);
+    gravtree_b200_drift();
     for (i = FirstActiveParticle; i >= 0; i = NextActiveParticle[i]) gg_active[n++] = i;
     for (i = 0; i < NumPart; i++) gg_oldacc[i] = P[i].OldAcc;
     gg_stats stats;

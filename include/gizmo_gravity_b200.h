@@ -132,6 +132,24 @@ gg_status gg_evaluate_device(gg_ctx *ctx, const int32_t *d_active, int64_t n_act
 /* interaction count and error word of the last evaluation (synchronises) */
 gg_status gg_last_stats(gg_ctx *ctx, gg_stats *stats);
 
+/* ---- drift of the resident tree ----------------------------------------
+ * Re-evaluation between rebuilds, as GIZMO does when TreeReconstructFlag is
+ * not set: particles move by Vel*dt (drift_particle, predict.c:97-137) and
+ * every node by force_drift_node (gravity/forcetree_update.c:265-338): centre
+ * of mass s += vs*dt, side len += 2*vmax*dt, geometric centre unchanged, with
+ * vs the node's mass-weighted mean velocity and vmax its largest |velocity
+ * component| (gravity/forcetree.c:558-560, :629, :751).  Velocities are per
+ * particle in load order (host arrays may be strided like the positions) and
+ * stay until the next load of particles.  gg_drift moves every system by dt;
+ * gg_drift_systems takes one dt per system (0 leaves a system where it is).
+ * Drifts accumulate; the next gg_build rebuilds at the drifted positions.
+ * Asynchronous on the context's stream (gg_drift_systems copies its host
+ * array before returning). */
+gg_status gg_load_velocities(gg_ctx *ctx, const double *vel, int64_t vel_stride_bytes);
+gg_status gg_load_velocities_device(gg_ctx *ctx, const double *d_vel);
+gg_status gg_drift(gg_ctx *ctx, double dt);
+gg_status gg_drift_systems(gg_ctx *ctx, const double *dt);
+
 /* ---- batched steps ------------------------------------------------------
  * No counterpart in the reference, which walks one system per process.  A
  * step of every resident system -- gg_build(ctx, NULL) then

@@ -186,6 +186,7 @@ static inline void pair_term(double dx, double dy, double dz, double r2, double 
 typedef struct {
     double center[3], len;
     double s[3], mass, maxsoft;
+    double vs[3], vmax;   /* mass-weighted mean velocity, largest |velocity component| (drift only) */
     int suns[8];   /* <n: particle, >=n: node n+idx, -1: empty */
     int multiple;  /* more than one particle below */
 } onode_t;
@@ -193,6 +194,7 @@ typedef struct {
 typedef struct {
     int64_t n;
     const double *pos, *mass, *h;
+    const double *vel;    /* NULL unless the tree is drifted */
     onode_t *nodes;
     int64_t nnodes, cap;
 } otree_t;
@@ -267,7 +269,7 @@ static void tree_build(otree_t *t, const double *center, const double *corner, d
 static void tree_moments(otree_t *t, int node)
 {
     onode_t *nd = &t->nodes[node];
-    double mass = 0, s[3] = {0, 0, 0}, maxsoft = 0;
+    double mass = 0, s[3] = {0, 0, 0}, maxsoft = 0, vs[3] = {0, 0, 0}, vmax = 0;
     int count = 0;
     for (int j = 0; j < 8; j++) {
         int p = t->nodes[node].suns[j];
@@ -279,6 +281,8 @@ static void tree_moments(otree_t *t, int node)
             onode_t *cn = &t->nodes[c];
             mass += cn->mass;
             for (int k = 0; k < 3; k++) s[k] += cn->mass * cn->s[k];
+            for (int k = 0; k < 3; k++) vs[k] += cn->mass * cn->vs[k];
+            if (cn->vmax > vmax) vmax = cn->vmax;
             if (cn->mass > 0) count += cn->multiple ? 2 : 1;
             if (cn->maxsoft > maxsoft) maxsoft = cn->maxsoft;
         } else {
@@ -286,11 +290,18 @@ static void tree_moments(otree_t *t, int node)
             mass += t->mass[p];
             for (int k = 0; k < 3; k++) s[k] += t->mass[p] * t->pos[3 * p + k];
             if (t->h[p] > maxsoft) maxsoft = t->h[p];
+            if (t->vel)
+                for (int k = 0; k < 3; k++) {
+                    vs[k] += t->mass[p] * t->vel[3 * p + k];
+                    if (fabs(t->vel[3 * p + k]) > vmax) vmax = fabs(t->vel[3 * p + k]);
+                }
         }
     }
-    if (mass) for (int k = 0; k < 3; k++) s[k] /= mass;
-    else for (int k = 0; k < 3; k++) s[k] = nd->center[k];
+    if (mass) for (int k = 0; k < 3; k++) { s[k] /= mass; vs[k] /= mass; }
+    else for (int k = 0; k < 3; k++) { s[k] = nd->center[k]; vs[k] = 0; }
     nd->mass = mass;
+    for (int k = 0; k < 3; k++) nd->vs[k] = vs[k];
+    nd->vmax = vmax;
     for (int k = 0; k < 3; k++) nd->s[k] = s[k];
     nd->maxsoft = maxsoft;
     nd->multiple = count > 1;
@@ -372,7 +383,7 @@ int64_t oracle_tree_gravity(int64_t n, const double *pos, const double *mass, co
 {
     double center[3], corner[3], len;
     oracle_find_extent(n, pos, center, corner, &len);
-    otree_t t = {n, pos, mass, h, NULL, 0, 0};
+    otree_t t = {n, pos, mass, h, NULL, NULL, 0, 0};
     tree_build(&t, center, corner, len);
     tree_moments(&t, 0);
     int64_t total = 0;
@@ -391,12 +402,59 @@ int64_t oracle_tree_gravity(int64_t n, const double *pos, const double *mass, co
     return total;
 }
 
+/*
+ * The same force after a drift of the resident tree without a rebuild: the
+ * tree is built and its moments taken at the positions `pos`, then every
+ * particle moves by vel*dt (drift_particle, predict.c:97-137) and every node
+ * by force_drift_node (forcetree_update.c:265-338): centre of mass
+ * s += vs*dt, side len += 2*vmax*dt, geometric centre unchanged, where vs is
+ * the mass-weighted mean velocity and vmax the largest |velocity component|
+ * of the node's particles (force_update_node_recursive, forcetree.c:558-560,
+ * :629, :751, :764-781).  Targets are evaluated at their drifted positions.
+ * pos_out (n*3, nullable) receives the drifted positions.
+ */
+int64_t oracle_tree_gravity_drift(int64_t n, const double *pos, const double *vel, const double *mass, const double *h,
+                                  const double *old_acc, double err_tol_force_acc, double err_tol_theta, double dt,
+                                  int64_t n_targets, const int32_t *targets, double *acc, double *pot, int64_t *ninter,
+                                  double *pos_out, int nthreads)
+{
+    double center[3], corner[3], len;
+    oracle_find_extent(n, pos, center, corner, &len);
+    otree_t t = {n, pos, mass, h, vel, NULL, 0, 0};
+    tree_build(&t, center, corner, len);
+    tree_moments(&t, 0);
+    for (int64_t k = 0; k < t.nnodes; k++) {
+        onode_t *nd = &t.nodes[k];
+        for (int j = 0; j < 3; j++) nd->s[j] += nd->vs[j] * dt;
+        nd->len += 2 * nd->vmax * dt;
+    }
+    double *moved = (double *)malloc(sizeof(double) * 3 * (n ? n : 1));
+    for (int64_t i = 0; i < 3 * n; i++) moved[i] = pos[i] + vel[i] * dt;
+    t.pos = moved;
+    int64_t total = 0;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : total)
+#endif
+    for (int64_t k = 0; k < n_targets; k++) {
+        int64_t i = targets ? targets[k] : k;
+        double aold = err_tol_force_acc * (old_acc ? old_acc[i] : 0.0);
+        int64_t c = tree_walk(&t, &moved[3 * i], h[i], aold, err_tol_theta, &acc[3 * k], &pot[k]);
+        if (ninter) ninter[k] = c;
+        total += c;
+    }
+    if (pos_out) memcpy(pos_out, moved, sizeof(double) * 3 * n);
+    free(moved);
+    free(t.nodes);
+    return total;
+}
+
 /* node count of the GIZMO octree (diagnostics) */
 int64_t oracle_tree_nodes(int64_t n, const double *pos, const double *mass, const double *h)
 {
     double center[3], corner[3], len;
     oracle_find_extent(n, pos, center, corner, &len);
-    otree_t t = {n, pos, mass, h, NULL, 0, 0};
+    otree_t t = {n, pos, mass, h, NULL, NULL, 0, 0};
     tree_build(&t, center, corner, len);
     int64_t m = t.nnodes;
     free(t.nodes);

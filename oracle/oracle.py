@@ -38,6 +38,8 @@ def lib():
         L.oracle_spline_gravity.restype = dbl
         L.oracle_tree_gravity.argtypes = [i64, P, P, P, P, dbl, dbl, i64, P, P, P, P, ctypes.c_int]
         L.oracle_tree_gravity.restype = i64
+        L.oracle_tree_gravity_drift.argtypes = [i64, P, P, P, P, P, dbl, dbl, dbl, i64, P, P, P, P, P, ctypes.c_int]
+        L.oracle_tree_gravity_drift.restype = i64
         L.oracle_tree_nodes.argtypes = [i64, P, P, P]
         L.oracle_tree_nodes.restype = i64
         L.oracle_direct_sum.argtypes = [i64, P, P, P, i64, P, P, P, ctypes.c_int]
@@ -93,6 +95,26 @@ def tree_gravity_two_pass(pos, mass, h, err_tol_force_acc=0.0025, err_tol_theta=
     a1, _, _, _ = tree_gravity(pos, mass, h, None, err_tol_force_acc, err_tol_theta, None, nthreads)
     old = np.linalg.norm(a1, axis=1)
     return tree_gravity(pos, mass, h, old, err_tol_force_acc, 0.0, targets, nthreads) + (old,)
+
+
+def tree_gravity_drift(pos, vel, mass, h, dt, old_acc=None, err_tol_force_acc=0.0025, err_tol_theta=0.0,
+                       targets=None, nthreads=0):
+    """Tree built at `pos`, then particles and nodes drifted by dt without a
+    rebuild (force_drift_node), then one pass at the drifted positions.
+    Returns acc (pre-G), pot, ninter, total, drifted positions."""
+    pos, vel = _c(pos, np.float64), _c(vel, np.float64)
+    mass, h = _c(mass, np.float64), _c(h, np.float64)
+    n = pos.shape[0]
+    tg = None if targets is None else _c(targets, np.int32)
+    nt = n if tg is None else tg.shape[0]
+    oa = None if old_acc is None else _c(old_acc, np.float64)
+    acc, pot, nint = np.zeros((nt, 3)), np.zeros(nt), np.zeros(nt, np.int64)
+    moved = np.zeros((n, 3))
+    total = lib().oracle_tree_gravity_drift(n, pos.ctypes.data, vel.ctypes.data, mass.ctypes.data, h.ctypes.data,
+                                            None if oa is None else oa.ctypes.data, err_tol_force_acc, err_tol_theta,
+                                            dt, nt, None if tg is None else tg.ctypes.data, acc.ctypes.data,
+                                            pot.ctypes.data, nint.ctypes.data, moved.ctypes.data, nthreads)
+    return acc, pot, nint, int(total), moved
 
 
 def tree_nodes(pos, mass, h):

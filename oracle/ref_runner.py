@@ -140,7 +140,7 @@ def types_and_eps(h):
 
 
 def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeout=3600, binary=None,
-        sample_only=False):
+        sample_only=False, drift_dt=0.0):
     """Run the reference: start-up evaluation (BH pass, relative pass) and
     optional steady-state steps.  Returns dict with acc (pre-G = acc/G with
     G = 1), pot, oldacc in input order, interaction counts and timings."""
@@ -159,8 +159,10 @@ def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeou
         with open(os.path.join(d, "params"), "w") as f:
             f.write(PARAMS.format(ic=icp, out=os.path.join(d, "out"), memmb=memmb, eps1=repr(eps1), eps2=repr(eps2)))
         args = [binary or BIN, os.path.join(d, "params"), repr(tol), os.path.join(d, "res.bin")]
-        if steps or sample is not None:
+        if steps or sample is not None or drift_dt > 0:
             args.append(str(steps))
+            if sample is None and drift_dt > 0:
+                args += ["-", "0"]
             if sample is not None:
                 sp = os.path.join(d, "sample.bin")
                 # IDs in the file are positions in the type-ordered file, plus one
@@ -168,8 +170,10 @@ def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeou
                 inv[order] = np.arange(n)
                 (inv[np.asarray(sample)] + 1).astype("<i8").tofile(sp)
                 args.append(sp)
-                if sample_only:
-                    args.append("1")
+                if sample_only or drift_dt > 0:
+                    args.append("1" if sample_only else "0")
+            if drift_dt > 0:
+                args.append(repr(float(drift_dt)))
         env = dict(os.environ)
         if threads:
             env["OMP_NUM_THREADS"] = str(threads)
@@ -192,7 +196,20 @@ def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeou
         keys_lo = np.empty(n, np.uint64)
         kidx = order[kr["id"].astype(np.int64) - 1]
         keys_hi[kidx], keys_lo[kidx] = kr["hi"], kr["lo"]
+        res_extra = {}
+        if drift_dt > 0:
+            dr = np.fromfile(os.path.join(d, "res.bin.drift"), dtype=rec.dtype)
+            out_dr = np.empty((n, 5))
+            out_dr[order[dr["id"].astype(np.int64) - 1]] = dr["v"]
+            pr = np.fromfile(os.path.join(d, "res.bin.pos"), dtype=np.dtype([("id", "<u8"), ("v", "<f8", 3)]))
+            pos_dr = np.empty((n, 3))
+            pos_dr[order[pr["id"].astype(np.int64) - 1]] = pr["v"]
+            res_extra = {"acc_drift": out_dr[:, :3], "pot_drift": out_dr[:, 3], "oldacc_drift": out_dr[:, 4],
+                         "pos_drift": pos_dr}
         for line in r.stdout.decode().splitlines():
+            if line.startswith("drift"):
+                kv = dict(p.split("=", 1) for p in line.split()[1:])
+                info["drift"] = {k: float(v) for k, v in kv.items()}
             if line.startswith("domain"):
                 kv = dict(p.split("=", 1) for p in line.split()[1:])
                 info["domain"] = {"corner": [float(x) for x in kv["corner"].split(",")], "len": float(kv["len"])}
@@ -204,7 +221,7 @@ def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeou
                 else:
                     info["steps"].append(kv)
         return {"acc": out[:, :3], "pot": out[:, 3], "oldacc": out[:, 4], "acc_bh": out_bh[:, :3],
-                "pot_bh": out_bh[:, 3], "key_hi": keys_hi, "key_lo": keys_lo, "info": info}
+                "pot_bh": out_bh[:, 3], "key_hi": keys_hi, "key_lo": keys_lo, "info": info, **res_extra}
     finally:
         if own:
             import shutil

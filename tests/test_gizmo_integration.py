@@ -6,7 +6,10 @@ construction and walk of gravity_tree() replaced by
 gizmo-public_b200/host/gravtree_b200.c, which hands GIZMO's own P[] records
 (strided) to the C ABI.  The same inputs go through the plain reference
 binary; results must agree to the tree's accuracy, with G applied and OldAcc
-set by the host code exactly as the reference's post-processing does.
+set by the host code exactly as the reference's post-processing does.  After
+the start-up passes, both binaries also re-evaluate the system a drift later
+without rebuilding the tree: the reference drifts its nodes inside the walk
+(force_drift_node), the host code drifts the device tree (gg_drift).
 """
 import numpy as np
 import pytest
@@ -26,8 +29,8 @@ def test_gizmo_with_b200_gravity_matches_reference(model):
         ic = ics.plummer(8192, seed=201)
     else:
         ic = ics.galaxy(n_halo=6000, n_disk=2192, seed=202)
-    ref = ref_runner.run(ic, threads=4)
-    gpu = ref_runner.run(ic, threads=4, binary=ref_runner.BIN_B200)
+    ref = ref_runner.run(ic, threads=4, drift_dt=0.002)
+    gpu = ref_runner.run(ic, threads=4, binary=ref_runner.BIN_B200, drift_dt=0.002)
     acc_d, pot_d = oracle.direct_sum(ic["pos"], ic["mass"], ic["h"])
     r50, r99, _ = ics.error_stats(ref["acc"], acc_d)
     g50, g99, _ = ics.error_stats(gpu["acc"], acc_d)
@@ -36,3 +39,10 @@ def test_gizmo_with_b200_gravity_matches_reference(model):
     assert np.allclose(gpu["oldacc"], np.linalg.norm(gpu["acc"], axis=1), rtol=1e-12)
     assert np.allclose(gpu["pot"], pot_d, rtol=2e-3)
     assert gpu["info"]["startup"]["cost_rel"] > 0
+    # the re-evaluation after the drift, against the direct sum at the drifted positions
+    assert gpu["info"]["drift"]["dt"] == ref["info"]["drift"]["dt"]
+    assert np.array_equal(gpu["pos_drift"], ref["pos_drift"])   # GIZMO's own particle drift in both
+    acc_dd, _ = oracle.direct_sum(ref["pos_drift"], ic["mass"], ic["h"])
+    r50, r99, _ = ics.error_stats(ref["acc_drift"], acc_dd)
+    g50, g99, _ = ics.error_stats(gpu["acc_drift"], acc_dd)
+    assert g50 <= 1.1 * r50 and g99 <= 1.1 * r99, (g50, g99, r50, r99)

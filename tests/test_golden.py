@@ -88,3 +88,52 @@ def test_gpu_default_mode_error_no_worse_than_reference(path):
     assert o50 <= 1.1 * r50 and o99 <= 1.1 * r99, (o50, o99, r50, r99)
     W, Wd, Wr = (0.5 * np.sum(g["mass"] * p) for p in (p2, pot_d, g["pot"]))
     assert abs(W - Wd) <= max(abs(Wr - Wd), 1e-5 * abs(Wd))
+
+
+# ---- re-evaluation after a drift without a rebuild (force_drift_node)
+@pytest.mark.parametrize("path", CASES, ids=IDS)
+def test_oracle_matches_reference_after_drift(path):
+    g = load(path)
+    tol, dt = float(g["tol"]), float(g["drift_dt"])
+    a, p, n, c, moved = oracle.tree_gravity_drift(g["pos"], g["vel"], g["mass"], g["h"], dt, old_acc=g["oldacc"],
+                                                  err_tol_force_acc=tol)
+    assert c == int(g["cost_drift"])
+    # the reference's compiler may fuse x + v*dt into one rounding: one unit in the last place
+    assert np.allclose(moved, g["pos_drift"], rtol=4e-16, atol=0)
+    assert np.allclose(a, g["acc_drift"], rtol=1e-12, atol=1e-14 * np.abs(g["acc_drift"]).max())
+    assert np.allclose(p, g["pot_drift"], rtol=1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", CASES, ids=IDS)
+def test_gpu_exact_mode_matches_reference_after_drift(path):
+    g = load(path)
+    tol, dt = float(g["tol"]), float(g["drift_dt"])
+    with ggb200.GravityTree(leaf_size=1, group_size=1) as t:
+        t.load(g["pos"], g["mass"], g["h"])
+        t.load_velocities(g["vel"])
+        t.build()
+        t.drift(dt)
+        a, p, n, s = t.evaluate(old_acc=g["oldacc"], err_tol_force_acc=tol, want_ninter=True)
+    assert abs(s["interactions"] - int(g["cost_drift"])) <= 8
+    rel = np.linalg.norm(a - g["acc_drift"], axis=1) / np.linalg.norm(g["acc_drift"], axis=1)
+    assert np.percentile(rel, 99) < 2e-5, np.percentile(rel, 99)
+    assert np.allclose(p, g["pot_drift"], rtol=5e-5)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", CASES, ids=IDS)
+def test_gpu_default_mode_after_drift_no_worse_than_reference(path):
+    g = load(path)
+    tol, dt = float(g["tol"]), float(g["drift_dt"])
+    acc_d, pot_d = oracle.direct_sum(g["pos_drift"], g["mass"], g["h"])
+    with ggb200.GravityTree() as t:
+        t.load(g["pos"], g["mass"], g["h"])
+        t.load_velocities(g["vel"])
+        t.build()
+        t.drift(dt)
+        a, p, _, s = t.evaluate(old_acc=g["oldacc"], err_tol_force_acc=tol)
+    r50, r99, _ = ics.error_stats(g["acc_drift"], acc_d)
+    o50, o99, _ = ics.error_stats(a, acc_d)
+    assert o50 <= 1.1 * r50 and o99 <= 1.1 * r99, (o50, o99, r50, r99)
+    assert s["error_word"] == 0
