@@ -214,29 +214,33 @@ def ensemble_direct(ic, d_pos, d_mass, d_h, counts, sys_of, idx, stream, dev):
     return acc
 
 
-def ensemble_reference_rate(ic, tol, n_sample=16, seed=77):
-    """The reference (compiled GIZMO, all host threads) run on a seeded sample
-    of whole systems of the ensemble, one process per system as it would run
-    them: particles/s = sum of N / sum of (domain + build + walk) step times."""
+def systems_reference_rate(systems, tol, what):
+    """The reference (compiled GIZMO, all host threads) run on whole systems,
+    one process per system as it would run them: particles/s = sum of N / sum
+    of (domain + build + walk) step times."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref_runner
     if not ref_runner.available():
         return None
-    counts = ic["counts"]
-    off = np.concatenate([[0], np.cumsum(counts)])
-    pick = np.sort(np.random.default_rng(seed).choice(counts.size, n_sample, replace=False))
     n_tot, t_tot, cores = 0, 0.0, os.cpu_count() or 1
-    for s in pick:
-        o, n = int(off[s]), int(counts[s])
-        sub = {k: ic[k][o:o + n] for k in ("pos", "vel", "mass", "h")}
+    for sub in systems:
+        n = int(sub["pos"].shape[0])
         rates, info = ref_runner.steps_rate(sub, steps=1, warmup=0, sample_n=n, tol=tol)
         n_tot += n
         t_tot += n / rates[0]
         cores = info["cores"]
     return {"value": n_tot / t_tot, "unit": "particles/s", "cores": cores, "kind": "reference",
             "sample": "GIZMO's own domain_Decomposition + tree build + relative walk (compiled reference, FP64, "
-                      "OpenMP %d threads), all particles active, on %d seeded whole systems of the ensemble "
-                      "(%d particles), one run per system" % (cores, n_sample, n_tot)}
+                      "OpenMP %d threads), all particles active, on %d seeded whole systems of the %s "
+                      "(%d particles), one run per system" % (cores, len(systems), what, n_tot)}
+
+
+def ensemble_reference_rate(ic, tol, n_sample=16, seed=77):
+    counts = ic["counts"]
+    off = np.concatenate([[0], np.cumsum(counts)])
+    pick = np.sort(np.random.default_rng(seed).choice(counts.size, n_sample, replace=False))
+    subs = [{k: ic[k][int(off[s]):int(off[s]) + int(counts[s])] for k in ("pos", "vel", "mass", "h")} for s in pick]
+    return systems_reference_rate(subs, tol, "ensemble")
 
 
 def run_ensemble(args, torch, ggb200, dist, world, rank, local):
@@ -414,6 +418,119 @@ def run_ensemble(args, torch, ggb200, dist, world, rank, local):
     return 0
 
 
+# ---------------------------------------------------------------- serving stream
+SERVE_NAME = "serve_poisson_2000rps_plummer_hernquist_clumpy_n1e3_1e6_reeval30"
+
+
+def _copy_trace(reqs):
+    import serve
+    return [serve.Request(r.rid, r.kind, r.arrival, system=r.system, target=r.target, dt=r.dt) for r in reqs]
+
+
+def run_serve(args, torch, ggb200, dist, world, rank, local):
+    """Poisson arrivals of force-evaluation solves, served with continuous
+    batching against a 120 GB device budget, then the same trace in the plain
+    one-request-at-a-time form."""
+    import serve
+    pool = ics.serving_pool(n_systems=128, seed=multi.rank_seed(ics.SEED_SERVING, rank))
+    trace = serve.make_trace(pool, rate=2000.0, window_s=args.serve_window, frac_reeval=0.3, dt=1e-3, recent=64,
+                             seed=multi.rank_seed(ics.SEED_SERVING, rank) + 1)
+    # warm-up: library, contexts and pinned staging on a short offline slice
+    warm = serve.Server(budget_bytes=120e9, tol=args.tol)
+    serve.run_trace(warm, _copy_trace(trace[:max(3, args.warmup) * 20]), realtime=False)
+    warm.close()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    launches0 = ggb200.kernel_launches()
+    srv = serve.Server(budget_bytes=120e9, tol=args.tol)
+    reqs = _copy_trace(trace)
+    wall = serve.run_trace(srv, reqs, realtime=True)
+    launches = ggb200.kernel_launches() - launches0
+    clk = clocks.stop()
+    st = serve.latency_stats(reqs)
+    st.update(batches=srv.n_batches, evictions=srv.evictions, misses=sum(r.miss for r in reqs),
+              peak_device_bytes=srv.peak_bytes, wall_s=wall)
+    srv.close()
+
+    plain = serve.Server(budget_bytes=120e9, tol=args.tol, batching=False)
+    preqs = _copy_trace(trace)
+    pwall = serve.run_trace(plain, preqs, realtime=True)
+    pst = serve.latency_stats(preqs)
+    pst.update(batches=plain.n_batches, evictions=plain.evictions, misses=sum(r.miss for r in preqs),
+               peak_device_bytes=plain.peak_bytes, wall_s=pwall)
+    plain.close()
+
+    # force error of a seeded sample of served results, FP64 direct sum at the served positions
+    dev = torch.device("cuda", local)
+    rng = np.random.default_rng(9)
+    errs, worst = [], 0.0
+    drift_acc = {}
+    for r in reqs:
+        sid = r.rid if r.kind == "new" else r.target
+        drift_acc[r.rid] = sum(q.dt for q in reqs if q.kind == "reeval" and q.target == sid and q.rid <= r.rid)
+    pick = rng.choice(len(reqs), min(24, len(reqs)), replace=False)
+    same_alone = 0
+    for i in pick:
+        r = reqs[i]
+        s = r.system if r.kind == "new" or r.miss else next(q.system for q in reqs if q.rid == r.target)
+        pos = s["pos"] + s["vel"] * drift_acc[r.rid] if drift_acc[r.rid] else s["pos"]
+        n = pos.shape[0]
+        ne = min(2048, n)
+        tg = np.sort(rng.choice(n, ne, replace=False)).astype(np.int32)
+        dp, dm, dh = (torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in (pos, s["mass"], s["h"]))
+        dacc = torch.empty((ne, 3), dtype=torch.float64, device=dev)
+        dpot = torch.empty(ne, dtype=torch.float64, device=dev)
+        ggb200.direct_sum_fp64(dp, dm, dh, n, torch.from_numpy(tg).to(dev), ne, dacc, dpot, None)
+        torch.cuda.synchronize()
+        _, p99, e = ics.error_stats(r.acc[tg], dacc.cpu().numpy())
+        errs.append(e)
+        worst = max(worst, p99)
+        # the same request in the plain form (alone): identical result
+        same_alone += int(np.array_equal(r.acc, preqs[i].acc))
+    e_all = np.concatenate(errs)
+
+    cpu = None
+    if not args.no_cpu and rank == 0 and world == 1:
+        small = sorted(pool, key=lambda x: x["pos"].shape[0])
+        cpu = systems_reference_rate([small[k] for k in range(0, 64, 8)], args.tol, "serving pool")
+
+    value = st["particles_per_s"]
+    n_req = st["requests"]
+    bytes_in = sum(r.n * (32 + 24) for r in reqs if r.kind == "new" or r.miss)
+    bytes_out = sum(r.n * 32 for r in reqs)
+    out = {
+        "metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world, "steps": n_req,
+        "warmup": args.warmup, "ms_per_step": 1e3 * st["makespan_s"] / n_req, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": SERVE_NAME, "rate_per_s": 2000.0, "window_s": args.serve_window, "requests": n_req,
+                   "reeval_fraction": 0.3, "drift_dt": 1e-3, "budget_bytes": 120e9, "err_tol_force_acc": args.tol,
+                   "pool_systems": len(pool), "step": "one request: arrival to result in host memory",
+                   "l2": "inputs streamed from host memory"},
+        "serve": st, "plain": pst,
+        "batched_vs_plain": {"particles_per_s_ratio": value / pst["particles_per_s"],
+                             "p50_ratio": pst["p50_ms"] / st["p50_ms"], "p99_ratio": pst["p99_ms"] / st["p99_ms"]},
+        "force_error": {"p50": float(np.median(e_all)), "p99": float(np.percentile(e_all, 99)),
+                        "worst_request_p99": worst, "requests_checked": int(pick.size),
+                        "same_as_plain": int(same_alone), "vs": "FP64 direct sum at the served positions"},
+        "clocks": clk, "gpu_launches": int(launches),
+        "e2e": {"value": value, "unit": "particles/s", "h2d_bytes_per_step": int(bytes_in / n_req),
+                "d2h_bytes_per_step": int(bytes_out / n_req),
+                "path": "serve.Server: gg_load_systems + gg_build + gg_evaluate_async / gg_drift_systems, "
+                        "results fetched to host memory"},
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
 # ---------------------------------------------------------------- GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -421,7 +538,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="galaxy", choices=sorted(WORKLOADS) + ["ensemble"])
+    ap.add_argument("--workload", default="galaxy", choices=sorted(WORKLOADS) + ["ensemble", "serve"])
     # 0.001 keeps the galaxy's p99 force error below 2e-3 (the metric's bound)
     ap.add_argument("--tol", type=float, default=0.001)
     ap.add_argument("--err-targets", type=int, default=65536)
@@ -435,6 +552,7 @@ def main():
     ap.add_argument("--flush", type=int, default=64)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--serve-window", type=float, default=2.0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -449,6 +567,8 @@ def main():
     dist = multi.init("nccl")
     if args.workload == "ensemble":
         return run_ensemble(args, torch, ggb200, dist, world, rank, local)
+    if args.workload == "serve":
+        return run_serve(args, torch, ggb200, dist, world, rank, local)
 
     name, gen = WORKLOADS[args.workload]
     ic = gen(multi.rank_seed(SEEDS[args.workload], rank))   # independent system per rank

@@ -127,7 +127,38 @@ struct gg_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     int graph_launches = 0;               // kernels inside the captured step
     bool have_events = false;
+    // host staging copies in flight: the next reuse of a staging buffer waits
+    // for its own copy only
+    cudaEvent_t stage_ev = nullptr, vstage_ev = nullptr;
+    // asynchronous evaluation: staged active list, pinned results, completion
+    int *h_active = nullptr;
+    size_t h_active_cap = 0;
+    double *h_acc = nullptr, *h_pot = nullptr;
+    size_t h_out_cap = 0;
+    long long async_n = 0;
+    int async_flags = 0;
+    cudaEvent_t act_ev = nullptr, done_ev = nullptr;
     gg_stats last;
+
+    // every device buffer of the context, for release and accounting
+    template <class F> void for_each_buf(F f)
+    {
+        f(poff); f(in_rec); f(part); f(dom); f(extent_mm); f(hmm); f(tkey); f(tval); f(tlist2); f(tout2);
+        f(keys); f(perm); f(rank); f(sort_scratch);
+        f(t_start); f(t_end); f(t_level); f(t_parent); f(t_sys); f(t_nch); f(t_child); f(t_counter); f(t_bnd);
+        f(t_depth); f(t_nnodes); f(t_bsum); f(t_boff); f(t_mass64); f(nodes);
+        f(oldacc); f(vel); f(kin); f(kin_counter); f(dts); f(oldacc_save);
+        f(groups); f(ngroups); f(gscan); f(toff); f(flag); f(flagscan); f(tlist); f(tout); f(scan_scratch);
+        f(active_d); f(counters); f(inter); f(stack); f(err); f(acc_d); f(pot_d); f(nint_d);
+    }
+};
+
+struct ReleaseBuf {
+    template <class B> void operator()(B &b) const { b.release(); }
+};
+struct CountBuf {
+    long long *total;
+    template <class B> void operator()(B &b) const { *total += (long long)(b.cap * sizeof(*b.p)); }
 };
 
 static gg_status set_device(gg_ctx *c)
@@ -150,6 +181,7 @@ extern "C" void gg_config_default(gg_config *cfg)
 extern "C" const char *gg_strerror(gg_status s)
 {
     switch (s) {
+    case GG_PENDING: return "pending";
     case GG_OK: return "ok";
     case GG_ERR_INVALID: return "invalid argument";
     case GG_ERR_CUDA: return g_last_cuda_error[0] ? g_last_cuda_error : "CUDA error";
@@ -187,6 +219,13 @@ extern "C" gg_status gg_create(const gg_config *cfg, gg_ctx **out)
     cudaError_t e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete ctx; return gg_cuda_fail(e); }
     ctx->stream = ctx->own_stream;
+    if ((e = cudaEventCreateWithFlags(&ctx->stage_ev, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->vstage_ev, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->act_ev, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->done_ev, cudaEventDisableTiming)) != cudaSuccess) {
+        gg_destroy(ctx);
+        return gg_cuda_fail(e);
+    }
     for (int i = 0; i < 8; i++) cudaEventCreate(&ctx->ev[i]);
     ctx->have_events = true;
     memset(&ctx->last, 0, sizeof ctx->last);
@@ -204,17 +243,14 @@ extern "C" gg_status gg_destroy(gg_ctx *c)
     if (!c) return GG_ERR_INVALID;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    c->poff.release(); c->in_rec.release(); c->part.release(); c->dom.release(); c->extent_mm.release(); c->hmm.release(); c->tkey.release(); c->tval.release();
-    c->tlist2.release(); c->tout2.release();
-    c->keys.release(); c->perm.release(); c->rank.release(); c->sort_scratch.release();
-    c->t_start.release(); c->t_end.release(); c->t_level.release(); c->t_parent.release(); c->t_sys.release();
-    c->t_nch.release(); c->t_child.release(); c->t_counter.release(); c->t_bnd.release(); c->t_depth.release();
-    c->t_nnodes.release(); c->t_bsum.release(); c->t_boff.release(); c->t_mass64.release(); c->nodes.release();
-    c->oldacc.release(); c->groups.release(); c->ngroups.release(); c->gscan.release(); c->toff.release();
-    c->flag.release(); c->flagscan.release(); c->tlist.release(); c->tout.release(); c->scan_scratch.release();
-    c->active_d.release(); c->counters.release(); c->inter.release(); c->stack.release(); c->err.release();
-    c->acc_d.release(); c->pot_d.release(); c->nint_d.release();
-    c->vel.release(); c->kin.release(); c->kin_counter.release(); c->dts.release(); c->oldacc_save.release();
+    c->for_each_buf(ReleaseBuf());
+    if (c->h_active) cudaFreeHost(c->h_active);
+    if (c->h_acc) cudaFreeHost(c->h_acc);
+    if (c->h_pot) cudaFreeHost(c->h_pot);
+    if (c->act_ev) cudaEventDestroy(c->act_ev);
+    if (c->done_ev) cudaEventDestroy(c->done_ev);
+    if (c->stage_ev) cudaEventDestroy(c->stage_ev);
+    if (c->vstage_ev) cudaEventDestroy(c->vstage_ev);
     if (c->h_vstage) cudaFreeHost(c->h_vstage);
     if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
@@ -283,13 +319,14 @@ extern "C" gg_status gg_load_particles(gg_ctx *c, int32_t S, const int64_t *coun
     if (soft_stride <= 0) soft_stride = sizeof(double);
     long long N = c->N;
     if ((size_t)N > c->h_stage_cap) {
+        GG_CUDA_TRY(cudaEventSynchronize(c->stage_ev));
         if (c->h_stage) cudaFreeHost(c->h_stage);
         c->h_stage = nullptr;
         c->h_stage_cap = 0;
         GG_CUDA_TRY(cudaMallocHost((void **)&c->h_stage, (size_t)(N ? N : 1) * sizeof(GGPart)));
         c->h_stage_cap = (size_t)(N ? N : 1);
     }
-    GG_CUDA_TRY(cudaStreamSynchronize(c->stream));   // staging buffer may still feed a previous copy
+    GG_CUDA_TRY(cudaEventSynchronize(c->stage_ev));   // the staging buffer may still feed the previous copy
     const char *pb = (const char *)pos, *mb = (const char *)mass, *hb = (const char *)soft_h;
     GGPart *dst = c->h_stage;
     int mixed = 0;
@@ -307,6 +344,7 @@ extern "C" gg_status gg_load_particles(gg_ctx *c, int32_t S, const int64_t *coun
     // systems also counts: harmless (ordering then just keeps each system's order)
     c->h_mixed = mixed != 0;
     if (N) GG_CUDA_TRY(cudaMemcpyAsync(c->in_rec.p, c->h_stage, N * sizeof(GGPart), cudaMemcpyHostToDevice, c->stream));
+    GG_CUDA_TRY(cudaEventRecord(c->stage_ev, c->stream));
     return GG_OK;
 }
 
@@ -790,13 +828,14 @@ extern "C" gg_status gg_load_velocities(gg_ctx *c, const double *vel, int64_t ve
     const long long N = c->N;
     if ((st = c->vel.ensure((size_t)3 * N + 3))) return st;
     if ((size_t)N > c->h_vstage_cap) {
+        GG_CUDA_TRY(cudaEventSynchronize(c->vstage_ev));
         if (c->h_vstage) cudaFreeHost(c->h_vstage);
         c->h_vstage = nullptr;
         c->h_vstage_cap = 0;
         GG_CUDA_TRY(cudaMallocHost((void **)&c->h_vstage, (size_t)(N ? N : 1) * 3 * sizeof(double)));
         c->h_vstage_cap = (size_t)(N ? N : 1);
     }
-    GG_CUDA_TRY(cudaStreamSynchronize(c->stream));   // staging buffer may still feed a previous copy
+    GG_CUDA_TRY(cudaEventSynchronize(c->vstage_ev));   // the staging buffer may still feed the previous copy
     const char *vb = (const char *)vel;
     double *dst = c->h_vstage;
 #pragma omp parallel for schedule(static)
@@ -805,6 +844,7 @@ extern "C" gg_status gg_load_velocities(gg_ctx *c, const double *vel, int64_t ve
         dst[3 * i] = v[0]; dst[3 * i + 1] = v[1]; dst[3 * i + 2] = v[2];
     }
     if (N) GG_CUDA_TRY(cudaMemcpyAsync(c->vel.p, dst, (size_t)N * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    GG_CUDA_TRY(cudaEventRecord(c->vstage_ev, c->stream));
     c->have_vel = true;
     c->kin_valid = false;
     return GG_OK;
@@ -864,4 +904,199 @@ extern "C" gg_status gg_drift_systems(gg_ctx *c, const double *dt)
 {
     if (!c || !dt) return GG_ERR_INVALID;
     return drift_common(c, dt, 0.0);
+}
+
+// ---------------------------------------------------------------- accounting
+extern "C" gg_status gg_device_bytes(gg_ctx *c, int64_t *bytes)
+{
+    if (!c || !bytes) return GG_ERR_INVALID;
+    long long total = 0;
+    c->for_each_buf(CountBuf{&total});
+    *bytes = (int64_t)total;
+    return GG_OK;
+}
+
+// ---------------------------------------------------------------- batches of separate host systems
+// Host gather of per-system arrays into the pinned staging buffer, in chunks
+// of at most 64K particles so that one large system spreads over the threads.
+struct HostChunk { int sys; long long first, count, dst; };
+
+static std::vector<HostChunk> host_chunks(const gg_ctx *c)
+{
+    std::vector<HostChunk> ch;
+    for (int s = 0; s < c->S; s++) {
+        const long long n = c->h_poff[s + 1] - c->h_poff[s];
+        for (long long f = 0; f < n; f += 65536)
+            ch.push_back({s, f, std::min(65536ll, n - f), (long long)c->h_poff[s] + f});
+    }
+    return ch;
+}
+
+static gg_status ensure_stage(gg_ctx *c)
+{
+    const long long N = c->N;
+    if ((size_t)N > c->h_stage_cap) {
+        GG_CUDA_TRY(cudaEventSynchronize(c->stage_ev));
+        if (c->h_stage) cudaFreeHost(c->h_stage);
+        c->h_stage = nullptr;
+        c->h_stage_cap = 0;
+        GG_CUDA_TRY(cudaMallocHost((void **)&c->h_stage, (size_t)(N ? N : 1) * sizeof(GGPart)));
+        c->h_stage_cap = (size_t)(N ? N : 1);
+    }
+    GG_CUDA_TRY(cudaEventSynchronize(c->stage_ev));   // the staging buffer may still feed the previous copy
+    return GG_OK;
+}
+
+extern "C" gg_status gg_load_systems(gg_ctx *c, int32_t S, const int64_t *counts, const double *const *pos,
+                                     const double *const *mass, const double *const *soft_h)
+{
+    if (!c || !pos || !mass || !soft_h || !counts || S < 1) return GG_ERR_INVALID;
+    for (int s = 0; s < S; s++)
+        if (counts[s] > 0 && (!pos[s] || !mass[s] || !soft_h[s])) return GG_ERR_INVALID;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    if ((st = set_systems(c, S, counts))) return st;
+    if ((st = ensure_stage(c))) return st;
+    const std::vector<HostChunk> ch = host_chunks(c);
+    GGPart *dst = c->h_stage;
+    int mixed = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(| : mixed)
+    for (long long k = 0; k < (long long)ch.size(); k++) {
+        const HostChunk q = ch[k];
+        const double *x = pos[q.sys], *m = mass[q.sys], *h = soft_h[q.sys];
+        const double h0 = h[0];
+        for (long long i = q.first; i < q.first + q.count; i++) {
+            GGPart r;
+            r.x = x[3 * i]; r.y = x[3 * i + 1]; r.z = x[3 * i + 2];
+            r.m = (float)m[i];
+            r.h = (float)h[i];
+            dst[q.dst + (i - q.first)] = r;
+            if ((float)h[i] != (float)h0) mixed = 1;
+        }
+    }
+    c->h_mixed = mixed != 0;
+    if (c->N) GG_CUDA_TRY(cudaMemcpyAsync(c->in_rec.p, c->h_stage, c->N * sizeof(GGPart), cudaMemcpyHostToDevice,
+                                          c->stream));
+    GG_CUDA_TRY(cudaEventRecord(c->stage_ev, c->stream));
+    return GG_OK;
+}
+
+extern "C" gg_status gg_load_system_velocities(gg_ctx *c, const double *const *vel)
+{
+    if (!c || !vel || c->S < 1) return GG_ERR_INVALID;
+    for (int s = 0; s < c->S; s++)
+        if (c->h_poff[s + 1] > c->h_poff[s] && !vel[s]) return GG_ERR_INVALID;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    const long long N = c->N;
+    if ((st = c->vel.ensure((size_t)3 * N + 3))) return st;
+    if ((size_t)N > c->h_vstage_cap) {
+        GG_CUDA_TRY(cudaEventSynchronize(c->vstage_ev));
+        if (c->h_vstage) cudaFreeHost(c->h_vstage);
+        c->h_vstage = nullptr;
+        c->h_vstage_cap = 0;
+        GG_CUDA_TRY(cudaMallocHost((void **)&c->h_vstage, (size_t)(N ? N : 1) * 3 * sizeof(double)));
+        c->h_vstage_cap = (size_t)(N ? N : 1);
+    }
+    GG_CUDA_TRY(cudaEventSynchronize(c->vstage_ev));
+    const std::vector<HostChunk> ch = host_chunks(c);
+    double *dst = c->h_vstage;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long k = 0; k < (long long)ch.size(); k++) {
+        const HostChunk q = ch[k];
+        memcpy(dst + 3 * q.dst, vel[q.sys] + 3 * q.first, (size_t)q.count * 3 * sizeof(double));
+    }
+    if (N) GG_CUDA_TRY(cudaMemcpyAsync(c->vel.p, dst, (size_t)N * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    GG_CUDA_TRY(cudaEventRecord(c->vstage_ev, c->stream));
+    c->have_vel = true;
+    c->kin_valid = false;
+    return GG_OK;
+}
+
+// ---------------------------------------------------------------- asynchronous evaluation
+extern "C" gg_status gg_evaluate_async(gg_ctx *c, const int32_t *active, int64_t n_active, double tol, double theta,
+                                       int32_t flags)
+{
+    if (!c) return GG_ERR_INVALID;
+    if (!c->built) return GG_ERR_NOT_BUILT;
+    if (tol < 0 || theta < 0 || (active && (n_active < 0 || n_active > c->N))) return GG_ERR_INVALID;
+    if (flags & ~(GG_ASYNC_COPY_ACC | GG_ASYNC_COPY_POT)) return GG_ERR_INVALID;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    cudaStream_t s = c->stream;
+    const long long nt = active ? n_active : c->N;
+    size_t outn = (size_t)(c->N > 0 ? c->N : 1);
+    if ((st = c->acc_d.ensure(outn * 3)) || (st = c->pot_d.ensure(outn))) return st;
+    const int *d_active = nullptr;
+    if (active) {
+        if ((size_t)n_active > c->h_active_cap) {
+            GG_CUDA_TRY(cudaEventSynchronize(c->act_ev));
+            if (c->h_active) cudaFreeHost(c->h_active);
+            c->h_active = nullptr;
+            c->h_active_cap = 0;
+            GG_CUDA_TRY(cudaMallocHost((void **)&c->h_active, (size_t)(n_active > 0 ? n_active : 1) * sizeof(int)));
+            c->h_active_cap = (size_t)(n_active > 0 ? n_active : 1);
+        }
+        GG_CUDA_TRY(cudaEventSynchronize(c->act_ev));
+        if ((st = c->active_d.ensure(n_active > 0 ? n_active : 1))) return st;
+        memcpy(c->h_active, active, (size_t)n_active * sizeof(int));
+        if (n_active)
+            GG_CUDA_TRY(cudaMemcpyAsync(c->active_d.p, c->h_active, n_active * sizeof(int), cudaMemcpyHostToDevice, s));
+        GG_CUDA_TRY(cudaEventRecord(c->act_ev, s));
+        d_active = c->active_d.p;
+    }
+    if ((st = run_walk(c, d_active, (int)n_active, nullptr, tol, theta, c->acc_d.p, c->pot_d.p, nullptr))) return st;
+    if (flags) {
+        if ((size_t)nt > c->h_out_cap) {
+            GG_CUDA_TRY(cudaEventSynchronize(c->done_ev));
+            if (c->h_acc) cudaFreeHost(c->h_acc);
+            if (c->h_pot) cudaFreeHost(c->h_pot);
+            c->h_acc = c->h_pot = nullptr;
+            c->h_out_cap = 0;
+            const size_t cap = (size_t)(nt > 0 ? nt : 1);
+            GG_CUDA_TRY(cudaMallocHost((void **)&c->h_acc, cap * 3 * sizeof(double)));
+            GG_CUDA_TRY(cudaMallocHost((void **)&c->h_pot, cap * sizeof(double)));
+            c->h_out_cap = cap;
+        } else {
+            // the previous results may not have been fetched yet: they are overwritten in stream order
+        }
+        if (nt && (flags & GG_ASYNC_COPY_ACC))
+            GG_CUDA_TRY(cudaMemcpyAsync(c->h_acc, c->acc_d.p, nt * 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (nt && (flags & GG_ASYNC_COPY_POT))
+            GG_CUDA_TRY(cudaMemcpyAsync(c->h_pot, c->pot_d.p, nt * sizeof(double), cudaMemcpyDeviceToHost, s));
+        c->async_n = nt;
+        c->async_flags = flags;
+    }
+    c->last.n_targets = nt;
+    GG_CUDA_TRY(cudaEventRecord(c->done_ev, s));
+    return GG_OK;
+}
+
+extern "C" gg_status gg_query(gg_ctx *c)
+{
+    if (!c) return GG_ERR_INVALID;
+    cudaError_t e = cudaEventQuery(c->done_ev);
+    if (e == cudaSuccess) return GG_OK;
+    if (e == cudaErrorNotReady) { cudaGetLastError(); return GG_PENDING; }
+    return gg_cuda_fail(e);
+}
+
+extern "C" gg_status gg_fetch_results(gg_ctx *c, double *acc_out, double *pot_out, gg_stats *stats)
+{
+    if (!c) return GG_ERR_INVALID;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    GG_CUDA_TRY(cudaEventSynchronize(c->done_ev));
+    const long long nt = c->async_n;
+    if (acc_out) {
+        if (!(c->async_flags & GG_ASYNC_COPY_ACC)) return GG_ERR_INVALID;
+        memcpy(acc_out, c->h_acc, (size_t)nt * 3 * sizeof(double));
+    }
+    if (pot_out) {
+        if (!(c->async_flags & GG_ASYNC_COPY_POT)) return GG_ERR_INVALID;
+        memcpy(pot_out, c->h_pot, (size_t)nt * sizeof(double));
+    }
+    st = collect_stats(c, stats);
+    if (stats) stats->n_targets = nt;
+    return st;
 }

@@ -22,6 +22,8 @@ LIB_PATH = os.path.join(HERE, "libgizmo_gravity_b200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "gizmo_gravity_b200.h")
 
 GG_OK = 0
+GG_PENDING = 1
+ASYNC_COPY_ACC, ASYNC_COPY_POT = 1, 2
 ERRORS = {
     -1: "GG_ERR_INVALID", -2: "GG_ERR_CUDA", -3: "GG_ERR_NOMEM", -4: "GG_ERR_OVERFLOW",
     -5: "GG_ERR_TIMEOUT", -6: "GG_ERR_NOT_BUILT", -7: "GG_ERR_BAD_INPUT", -8: "GG_ERR_TOO_LARGE",
@@ -115,6 +117,12 @@ def load_library():
             "gg_load_velocities": (i32, [P, P, i64]),
             "gg_load_velocities_device": (i32, [P, P]),
             "gg_drift": (i32, [P, dbl]),
+            "gg_device_bytes": (i32, [P, ctypes.POINTER(i64)]),
+            "gg_load_systems": (i32, [P, i32, P, P, P, P]),
+            "gg_load_system_velocities": (i32, [P, P]),
+            "gg_evaluate_async": (i32, [P, P, i64, dbl, dbl, i32]),
+            "gg_query": (i32, [P]),
+            "gg_fetch_results": (i32, [P, P, P, ctypes.POINTER(Stats)]),
             "gg_drift_systems": (i32, [P, P]),
             "gg_graph_capture_step": (i32, [P, dbl, dbl, P, P]),
             "gg_graph_launch": (i32, [P]),
@@ -263,6 +271,57 @@ class GravityTree:
             _check(self._lib.gg_load_velocities(self._h, v.ctypes.data, 24), "gg_load_velocities")
         else:
             _check(self._lib.gg_load_velocities_device(self._h, _ptr(vel)), "gg_load_velocities_device")
+
+    def load_systems(self, systems):
+        """Load independent systems given as separate arrays: a sequence of
+        dicts with pos (n,3), mass (n), h (n) and optionally vel (n,3)."""
+        arrs = [(np.ascontiguousarray(x["pos"], dtype=np.float64), np.ascontiguousarray(x["mass"], dtype=np.float64),
+                 np.ascontiguousarray(x["h"], dtype=np.float64)) for x in systems]
+        S = len(arrs)
+        counts = np.array([a[0].shape[0] for a in arrs], dtype=np.int64)
+        ptrs = [(ctypes.c_void_p * S)(*[a[k].ctypes.data for a in arrs]) for k in range(3)]
+        _check(self._lib.gg_load_systems(self._h, S, counts.ctypes.data, ptrs[0], ptrs[1], ptrs[2]), "gg_load_systems")
+        self.n, self.counts = int(counts.sum()), counts
+        self._keep = (arrs, ptrs, counts)
+        if all("vel" in x for x in systems):
+            vs = [np.ascontiguousarray(x["vel"], dtype=np.float64) for x in systems]
+            vp = (ctypes.c_void_p * S)(*[v.ctypes.data for v in vs])
+            _check(self._lib.gg_load_system_velocities(self._h, vp), "gg_load_system_velocities")
+            self._keepv = (vs, vp)
+
+    def evaluate_async(self, active=None, err_tol_force_acc=0.0025, err_tol_theta=0.0, copy_acc=True,
+                       copy_pot=True):
+        """Queue a walk (and the copy of its results to pinned host memory); returns at once."""
+        act = None if active is None else np.ascontiguousarray(active, dtype=np.int32)
+        flags = (ASYNC_COPY_ACC if copy_acc else 0) | (ASYNC_COPY_POT if copy_pot else 0)
+        n = 0 if act is None else act.shape[0]
+        _check(self._lib.gg_evaluate_async(self._h, None if act is None else act.ctypes.data, n, err_tol_force_acc,
+                                           err_tol_theta, flags), "gg_evaluate_async")
+        self._async_n = self.n if act is None else n
+        self._async_flags = flags
+
+    def query(self):
+        """True when the last asynchronous evaluation has finished."""
+        st = self._lib.gg_query(self._h)
+        if st == GG_PENDING:
+            return False
+        _check(st, "gg_query")
+        return True
+
+    def fetch(self):
+        """Wait for the last asynchronous evaluation; returns (acc, pot, stats)."""
+        n = self._async_n
+        acc = np.empty((n, 3)) if self._async_flags & ASYNC_COPY_ACC else None
+        pot = np.empty(n) if self._async_flags & ASYNC_COPY_POT else None
+        st = Stats()
+        _check(self._lib.gg_fetch_results(self._h, _ptr(acc), _ptr(pot), ctypes.byref(st)), "gg_fetch_results")
+        return acc, pot, st.as_dict()
+
+    def device_bytes(self):
+        """Device memory the context holds now."""
+        v = ctypes.c_int64()
+        _check(self._lib.gg_device_bytes(self._h, ctypes.byref(v)), "gg_device_bytes")
+        return v.value
 
     def drift(self, dt):
         """Move particles and nodes of the resident tree by dt (a number), or by

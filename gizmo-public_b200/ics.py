@@ -110,9 +110,9 @@ def galaxy(n_halo=3_000_000, n_disk=1_194_304, seed=SEED_GALAXY, eps_halo=0.01, 
     dvel = np.stack([-vc * np.sin(phi), vc * np.cos(phi), np.zeros(n_disk)], axis=1)
     pos = np.concatenate([hpos, dpos])
     vel = np.concatenate([hvel, dvel])
-    mass = np.concatenate([np.full(n_halo, m_halo / n_halo), np.full(n_disk, m_disk / n_disk)])
+    mass = np.concatenate([np.full(n_halo, m_halo / n_halo), np.full(n_disk, m_disk / max(n_disk, 1))])
     h = np.concatenate([np.full(n_halo, KERNEL_FAC * eps_halo), np.full(n_disk, KERNEL_FAC * eps_disk)])
-    ratio = (m_disk / n_disk) / (m_halo / n_halo)
+    ratio = (m_disk / n_disk) / (m_halo / n_halo) if n_disk else None
     return dict(pos=pos, vel=vel, mass=mass, h=h,
                 meta=dict(model="galaxy", n=n_halo + n_disk, n_halo=n_halo, n_disk=n_disk, seed=seed,
                           eps_halo=eps_halo, eps_disk=eps_disk, halo_rmax=100.0, rd=rd, z0=z0,
@@ -251,6 +251,30 @@ def ensemble(n_systems=4096, nmin=256, nmax=65536, seed=SEED_ENSEMBLE):
                 h=np.concatenate(h_l), counts=sizes, kinds=kinds,
                 meta=dict(model="ensemble", n_systems=n_systems, nmin=nmin, nmax=nmax, seed=seed,
                           total=int(sizes.sum()), eps="0.01 r_half"))
+
+
+def serving_system(kind, n, seed):
+    """One system of a serving stream: 0 Plummer (eps 0.01), 1 Hernquist halo
+    (eps 0.01), 2 clumpy mixture (Plummer clumps plus background, eps 1e-4)."""
+    if kind == 0:
+        return plummer(n, seed=seed)
+    if kind == 1:
+        return galaxy(n_halo=n, n_disk=0, seed=seed)
+    return clustered(n, seed=seed, n_clumps=int(max(4, min(100, n // 1000))))
+
+
+def serving_pool(n_systems=64, nmin=1000, nmax=1_000_000, seed=SEED_SERVING):
+    """Systems for a serving stream: sizes log-uniform in [nmin, nmax], kinds
+    Plummer / Hernquist / clumpy in equal shares, each from its own seed."""
+    rng = _rng(seed)
+    sizes = np.exp(rng.uniform(np.log(nmin), np.log(nmax), n_systems)).astype(np.int64)
+    kinds = rng.integers(0, 3, n_systems)
+    pool = []
+    for i in range(n_systems):
+        s = serving_system(int(kinds[i]), int(sizes[i]), seed + 1 + i)
+        s["kind"] = int(kinds[i])
+        pool.append(s)
+    return pool
 
 
 def error_stats(acc, acc_ref):

@@ -37,6 +37,7 @@ extern "C" {
 typedef int32_t gg_status;
 
 enum {
+    GG_PENDING = 1,           /* gg_query: the context's last asynchronous work is still running */
     GG_OK = 0,
     GG_ERR_INVALID = -1,      /* bad argument (null pointer, negative size, ...) */
     GG_ERR_CUDA = -2,         /* CUDA runtime error or no usable device */
@@ -132,6 +133,10 @@ gg_status gg_evaluate_device(gg_ctx *ctx, const int32_t *d_active, int64_t n_act
 /* interaction count and error word of the last evaluation (synchronises) */
 gg_status gg_last_stats(gg_ctx *ctx, gg_stats *stats);
 
+/* device memory the context holds now (all its buffers), for callers that
+ * admit work against a memory budget; no counterpart in the reference */
+gg_status gg_device_bytes(gg_ctx *ctx, int64_t *bytes);
+
 /* ---- drift of the resident tree ----------------------------------------
  * Re-evaluation between rebuilds, as GIZMO does when TreeReconstructFlag is
  * not set: particles move by Vel*dt (drift_particle, predict.c:97-137) and
@@ -149,6 +154,29 @@ gg_status gg_load_velocities(gg_ctx *ctx, const double *vel, int64_t vel_stride_
 gg_status gg_load_velocities_device(gg_ctx *ctx, const double *d_vel);
 gg_status gg_drift(gg_ctx *ctx, double dt);
 gg_status gg_drift_systems(gg_ctx *ctx, const double *dt);
+
+/* ---- batches of independent systems and asynchronous evaluation ----------
+ * No counterpart in the reference, which holds one system per process.
+ * gg_load_systems loads n_systems systems given as separate host arrays (one
+ * pointer per system to its n*3 positions, n masses and n kernel radii),
+ * gathered directly into the context's pinned staging buffer; the copy to the
+ * device is asynchronous.  gg_load_system_velocities does the same for the
+ * velocities the drift needs.
+ * gg_evaluate_async queues the walk of `active` (host indices in load order,
+ * NULL = all) and, per flags, the copy of the results into pinned buffers of
+ * the context; it returns without waiting.  gg_query returns GG_PENDING while
+ * that work runs and GG_OK when it is done; gg_fetch_results waits for it and
+ * copies acc (n*3) and pot (n) out (nullable each) with the stats.  A later
+ * gg_evaluate_async of the same context overwrites unfetched results. */
+#define GG_ASYNC_COPY_ACC 1
+#define GG_ASYNC_COPY_POT 2
+gg_status gg_load_systems(gg_ctx *ctx, int32_t n_systems, const int64_t *counts, const double *const *pos,
+                          const double *const *mass, const double *const *soft_h);
+gg_status gg_load_system_velocities(gg_ctx *ctx, const double *const *vel);
+gg_status gg_evaluate_async(gg_ctx *ctx, const int32_t *active, int64_t n_active, double err_tol_force_acc,
+                            double err_tol_theta, int32_t flags);
+gg_status gg_query(gg_ctx *ctx);
+gg_status gg_fetch_results(gg_ctx *ctx, double *acc_out, double *pot_out, gg_stats *stats);
 
 /* ---- batched steps ------------------------------------------------------
  * No counterpart in the reference, which walks one system per process.  A
