@@ -436,8 +436,8 @@ def run_serve(args, torch, ggb200, dist, world, rank, local):
     trace = serve.make_trace(pool, rate=2000.0, window_s=args.serve_window, frac_reeval=0.3, dt=1e-3, recent=64,
                              seed=multi.rank_seed(ics.SEED_SERVING, rank) + 1)
     # warm-up: library, contexts and pinned staging on a short offline slice
-    warm = serve.Server(budget_bytes=120e9, tol=args.tol)
-    serve.run_trace(warm, _copy_trace(trace[:max(3, args.warmup) * 20]), realtime=False)
+    warm = serve.Server(budget_bytes=120e9, tol=args.tol, reserve=True)   # maps the 120 GB budget once
+    serve.run_trace(warm, _copy_trace(trace[:max(3, args.warmup) * 100]), realtime=False)
     warm.close()
     torch.cuda.synchronize()
 
@@ -447,7 +447,7 @@ def run_serve(args, torch, ggb200, dist, world, rank, local):
     if dist:
         dist.barrier()
     launches0 = ggb200.kernel_launches()
-    srv = serve.Server(budget_bytes=120e9, tol=args.tol)
+    srv = serve.Server(budget_bytes=120e9, tol=args.tol, reserve=True)
     reqs = _copy_trace(trace)
     wall = serve.run_trace(srv, reqs, realtime=True)
     launches = ggb200.kernel_launches() - launches0
@@ -457,7 +457,7 @@ def run_serve(args, torch, ggb200, dist, world, rank, local):
               peak_device_bytes=srv.peak_bytes, wall_s=wall)
     srv.close()
 
-    plain = serve.Server(budget_bytes=120e9, tol=args.tol, batching=False)
+    plain = serve.Server(budget_bytes=120e9, tol=args.tol, batching=False, reserve=True)
     preqs = _copy_trace(trace)
     pwall = serve.run_trace(plain, preqs, realtime=True)
     pst = serve.latency_stats(preqs)

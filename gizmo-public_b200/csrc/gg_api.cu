@@ -5,6 +5,9 @@
 
 #include <algorithm>
 #include <atomic>
+#include <iterator>
+#include <map>
+#include <mutex>
 #include <cmath>
 #include <vector>
 
@@ -40,27 +43,118 @@ int gg_num_sms()
     return cached[dev];
 }
 
+// Device buffers are allocated in stream order on the context's stream
+// (cudaMallocAsync / cudaFreeAsync from the device's default pool, which keeps
+// freed memory cached), so creating, growing or destroying a context never
+// waits for the whole device.  Contents are not kept across a growth.
 template <typename T>
 struct DevBuf {
     T *p = nullptr;
     size_t cap = 0;
+    const cudaStream_t *sref = nullptr;   // the owning context's current stream
     gg_status ensure(size_t n)
     {
         if (n <= cap && p) return GG_OK;
-        if (p) cudaFree(p);
+        const cudaStream_t s = sref ? *sref : (cudaStream_t)0;
+        if (p) cudaFreeAsync(p, s);
         p = nullptr;
         cap = 0;
         size_t want = n < 1 ? 1 : n;
-        cudaError_t e = cudaMalloc((void **)&p, want * sizeof(T));
-        if (e != cudaSuccess) return gg_cuda_fail(e);
+        cudaError_t e = cudaMallocAsync((void **)&p, want * sizeof(T), s);
+        if (e != cudaSuccess) { p = nullptr; return gg_cuda_fail(e); }
         cap = want;
         return GG_OK;
     }
     void release()
     {
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, sref ? *sref : (cudaStream_t)0);
         p = nullptr;
         cap = 0;
+    }
+};
+
+// Pinned host blocks shared by every context of the process: host staging of
+// particle loads, active lists and results is borrowed for the duration of a
+// transfer and given back, so a new context does not page-lock memory again.
+// Blocks come in power-of-two sizes from 1 MB, so that a block given back
+// serves any later request of its size class; they are kept for reuse up to
+// kPinnedCacheBytes in total.
+static const size_t kPinnedCacheBytes = (size_t)16 << 30;
+static std::mutex g_pinned_mu;
+static std::multimap<size_t, void *> g_pinned_free;
+static size_t g_pinned_cached = 0;
+
+static size_t pinned_class(size_t bytes)
+{
+    size_t c = (size_t)1 << 20;
+    while (c < bytes) c <<= 1;
+    return c;
+}
+
+static void *pinned_get(size_t bytes, size_t *got)
+{
+    const size_t want = pinned_class(bytes);
+    {
+        std::lock_guard<std::mutex> lk(g_pinned_mu);
+        auto it = g_pinned_free.find(want);
+        if (it != g_pinned_free.end()) {
+            void *p = it->second;
+            *got = it->first;
+            g_pinned_cached -= it->first;
+            g_pinned_free.erase(it);
+            return p;
+        }
+    }
+    void *p = nullptr;
+    if (cudaHostAlloc(&p, want, cudaHostAllocPortable) != cudaSuccess) return nullptr;
+    *got = want;
+    return p;
+}
+
+static void pinned_put(void *p, size_t bytes)
+{
+    if (!p) return;
+    std::vector<void *> drop;
+    {
+        std::lock_guard<std::mutex> lk(g_pinned_mu);
+        g_pinned_free.emplace(bytes, p);
+        g_pinned_cached += bytes;
+        while (g_pinned_cached > kPinnedCacheBytes && !g_pinned_free.empty()) {
+            auto it = std::prev(g_pinned_free.end());
+            g_pinned_cached -= it->first;
+            drop.push_back(it->second);
+            g_pinned_free.erase(it);
+        }
+    }
+    for (void *q : drop) cudaFreeHost(q);
+}
+
+// A pinned host buffer borrowed from the pool; `guard` is the event recorded
+// after the last transfer that reads or writes it.
+template <typename T>
+struct HostBuf {
+    T *p = nullptr;
+    size_t cap = 0, bytes = 0;
+    gg_status ensure(size_t n, cudaEvent_t guard)
+    {
+        if (n <= cap && p) {
+            GG_CUDA_TRY(cudaEventSynchronize(guard));   // may still feed the previous transfer
+            return GG_OK;
+        }
+        give_back(guard);
+        size_t want = n < 1 ? 1 : n;
+        p = (T *)pinned_get(want * sizeof(T), &bytes);
+        if (!p) { bytes = 0; return GG_ERR_NOMEM; }
+        cap = bytes / sizeof(T);
+        return GG_OK;
+    }
+    void give_back(cudaEvent_t guard)
+    {
+        if (!p) return;
+        if (guard) cudaEventSynchronize(guard);
+        pinned_put(p, bytes);
+        p = nullptr;
+        cap = bytes = 0;
     }
 };
 
@@ -104,8 +198,7 @@ struct gg_ctx {
     bool kin_valid = false;
     bool kin_any = false;                  // kinematics computed at least once for this build
     DevBuf<double> dts;
-    double *h_vstage = nullptr;
-    size_t h_vstage_cap = 0;
+    HostBuf<double> h_vstage;
     DevBuf<double> oldacc_save;           // autotuner: every trial starts from the same OldAcc
     bool oldacc_valid = false;
     DevBuf<GGGroup> groups;
@@ -118,8 +211,7 @@ struct gg_ctx {
     DevBuf<int> nint_d;
     int walk_blocks = 0;
     // host staging
-    GGPart *h_stage = nullptr;
-    size_t h_stage_cap = 0;
+    HostBuf<GGPart> h_stage;
     // timing
     cudaEvent_t ev[8];
     // a captured step (build + walk) replayed as one CUDA graph
@@ -131,10 +223,8 @@ struct gg_ctx {
     // for its own copy only
     cudaEvent_t stage_ev = nullptr, vstage_ev = nullptr;
     // asynchronous evaluation: staged active list, pinned results, completion
-    int *h_active = nullptr;
-    size_t h_active_cap = 0;
-    double *h_acc = nullptr, *h_pot = nullptr;
-    size_t h_out_cap = 0;
+    HostBuf<int> h_active;
+    HostBuf<double> h_acc, h_pot;
     long long async_n = 0;
     int async_flags = 0;
     cudaEvent_t act_ev = nullptr, done_ev = nullptr;
@@ -195,6 +285,24 @@ extern "C" const char *gg_strerror(gg_status s)
     }
 }
 
+// Keep memory freed by contexts cached in the device's default pool for the
+// next context (the default threshold hands it back to the driver at every
+// synchronisation).  A property of this process's pool only.
+static void keep_pool_memory(int device)
+{
+    static std::mutex mu;
+    static bool done[64] = {false};
+    std::lock_guard<std::mutex> lk(mu);
+    if (device < 0 || device >= 64 || done[device]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    cudaGetLastError();
+    done[device] = true;
+}
+
 extern "C" gg_status gg_create(const gg_config *cfg, gg_ctx **out)
 {
     if (!out) return GG_ERR_INVALID;
@@ -219,6 +327,8 @@ extern "C" gg_status gg_create(const gg_config *cfg, gg_ctx **out)
     cudaError_t e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete ctx; return gg_cuda_fail(e); }
     ctx->stream = ctx->own_stream;
+    ctx->for_each_buf([ctx](auto &b) { b.sref = &ctx->stream; });
+    keep_pool_memory(ctx->device);
     if ((e = cudaEventCreateWithFlags(&ctx->stage_ev, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&ctx->vstage_ev, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&ctx->act_ev, cudaEventDisableTiming)) != cudaSuccess ||
@@ -244,15 +354,15 @@ extern "C" gg_status gg_destroy(gg_ctx *c)
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->for_each_buf(ReleaseBuf());
-    if (c->h_active) cudaFreeHost(c->h_active);
-    if (c->h_acc) cudaFreeHost(c->h_acc);
-    if (c->h_pot) cudaFreeHost(c->h_pot);
+    c->h_active.give_back(c->act_ev);
+    c->h_acc.give_back(c->done_ev);
+    c->h_pot.give_back(c->done_ev);
+    c->h_vstage.give_back(c->vstage_ev);
+    c->h_stage.give_back(c->stage_ev);
     if (c->act_ev) cudaEventDestroy(c->act_ev);
     if (c->done_ev) cudaEventDestroy(c->done_ev);
     if (c->stage_ev) cudaEventDestroy(c->stage_ev);
     if (c->vstage_ev) cudaEventDestroy(c->vstage_ev);
-    if (c->h_vstage) cudaFreeHost(c->h_vstage);
-    if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     if (c->have_events)
@@ -265,6 +375,11 @@ extern "C" gg_status gg_destroy(gg_ctx *c)
 extern "C" gg_status gg_set_stream(gg_ctx *c, void *s)
 {
     if (!c) return GG_ERR_INVALID;
+    if (c->stream != (cudaStream_t)s) {
+        // buffers are freed in stream order: finish what the old stream may still do with them
+        cudaSetDevice(c->device);
+        GG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    }
     c->stream = (cudaStream_t)s;   // NULL is the legacy default stream, as for any CUDA call
     return GG_OK;
 }
@@ -318,17 +433,9 @@ extern "C" gg_status gg_load_particles(gg_ctx *c, int32_t S, const int64_t *coun
     if (mass_stride <= 0) mass_stride = sizeof(double);
     if (soft_stride <= 0) soft_stride = sizeof(double);
     long long N = c->N;
-    if ((size_t)N > c->h_stage_cap) {
-        GG_CUDA_TRY(cudaEventSynchronize(c->stage_ev));
-        if (c->h_stage) cudaFreeHost(c->h_stage);
-        c->h_stage = nullptr;
-        c->h_stage_cap = 0;
-        GG_CUDA_TRY(cudaMallocHost((void **)&c->h_stage, (size_t)(N ? N : 1) * sizeof(GGPart)));
-        c->h_stage_cap = (size_t)(N ? N : 1);
-    }
-    GG_CUDA_TRY(cudaEventSynchronize(c->stage_ev));   // the staging buffer may still feed the previous copy
+    if ((st = c->h_stage.ensure((size_t)N, c->stage_ev))) return st;
     const char *pb = (const char *)pos, *mb = (const char *)mass, *hb = (const char *)soft_h;
-    GGPart *dst = c->h_stage;
+    GGPart *dst = c->h_stage.p;
     int mixed = 0;
 #pragma omp parallel for schedule(static) reduction(| : mixed)
     for (long long i = 0; i < N; i++) {
@@ -343,7 +450,7 @@ extern "C" gg_status gg_load_particles(gg_ctx *c, int32_t S, const int64_t *coun
     // a change of kernel radius between neighbouring particles of different
     // systems also counts: harmless (ordering then just keeps each system's order)
     c->h_mixed = mixed != 0;
-    if (N) GG_CUDA_TRY(cudaMemcpyAsync(c->in_rec.p, c->h_stage, N * sizeof(GGPart), cudaMemcpyHostToDevice, c->stream));
+    if (N) GG_CUDA_TRY(cudaMemcpyAsync(c->in_rec.p, c->h_stage.p, N * sizeof(GGPart), cudaMemcpyHostToDevice, c->stream));
     GG_CUDA_TRY(cudaEventRecord(c->stage_ev, c->stream));
     return GG_OK;
 }
@@ -635,6 +742,8 @@ extern "C" gg_status gg_evaluate(gg_ctx *c, const int32_t *active, int64_t n_act
         GG_CUDA_TRY(cudaMemcpyAsync(ni.data(), c->nint_d.p, nt * sizeof(int), cudaMemcpyDeviceToHost, s));
     }
     st = collect_stats(c, stats);
+    c->h_stage.give_back(c->stage_ev);     // the loads before this evaluation are complete
+    c->h_vstage.give_back(c->vstage_ev);
     if (ninter_out)
         for (long long i = 0; i < nt; i++) ninter_out[i] = ni[i];
     c->last.n_targets = nt;
@@ -827,17 +936,9 @@ extern "C" gg_status gg_load_velocities(gg_ctx *c, const double *vel, int64_t ve
     if (vel_stride <= 0) vel_stride = 3 * sizeof(double);
     const long long N = c->N;
     if ((st = c->vel.ensure((size_t)3 * N + 3))) return st;
-    if ((size_t)N > c->h_vstage_cap) {
-        GG_CUDA_TRY(cudaEventSynchronize(c->vstage_ev));
-        if (c->h_vstage) cudaFreeHost(c->h_vstage);
-        c->h_vstage = nullptr;
-        c->h_vstage_cap = 0;
-        GG_CUDA_TRY(cudaMallocHost((void **)&c->h_vstage, (size_t)(N ? N : 1) * 3 * sizeof(double)));
-        c->h_vstage_cap = (size_t)(N ? N : 1);
-    }
-    GG_CUDA_TRY(cudaEventSynchronize(c->vstage_ev));   // the staging buffer may still feed the previous copy
+    if ((st = c->h_vstage.ensure((size_t)N * 3, c->vstage_ev))) return st;
     const char *vb = (const char *)vel;
-    double *dst = c->h_vstage;
+    double *dst = c->h_vstage.p;
 #pragma omp parallel for schedule(static)
     for (long long i = 0; i < N; i++) {
         const double *v = (const double *)(vb + i * vel_stride);
@@ -934,17 +1035,7 @@ static std::vector<HostChunk> host_chunks(const gg_ctx *c)
 
 static gg_status ensure_stage(gg_ctx *c)
 {
-    const long long N = c->N;
-    if ((size_t)N > c->h_stage_cap) {
-        GG_CUDA_TRY(cudaEventSynchronize(c->stage_ev));
-        if (c->h_stage) cudaFreeHost(c->h_stage);
-        c->h_stage = nullptr;
-        c->h_stage_cap = 0;
-        GG_CUDA_TRY(cudaMallocHost((void **)&c->h_stage, (size_t)(N ? N : 1) * sizeof(GGPart)));
-        c->h_stage_cap = (size_t)(N ? N : 1);
-    }
-    GG_CUDA_TRY(cudaEventSynchronize(c->stage_ev));   // the staging buffer may still feed the previous copy
-    return GG_OK;
+    return c->h_stage.ensure((size_t)c->N, c->stage_ev);
 }
 
 extern "C" gg_status gg_load_systems(gg_ctx *c, int32_t S, const int64_t *counts, const double *const *pos,
@@ -958,7 +1049,7 @@ extern "C" gg_status gg_load_systems(gg_ctx *c, int32_t S, const int64_t *counts
     if ((st = set_systems(c, S, counts))) return st;
     if ((st = ensure_stage(c))) return st;
     const std::vector<HostChunk> ch = host_chunks(c);
-    GGPart *dst = c->h_stage;
+    GGPart *dst = c->h_stage.p;
     int mixed = 0;
 #pragma omp parallel for schedule(dynamic, 1) reduction(| : mixed)
     for (long long k = 0; k < (long long)ch.size(); k++) {
@@ -975,7 +1066,7 @@ extern "C" gg_status gg_load_systems(gg_ctx *c, int32_t S, const int64_t *counts
         }
     }
     c->h_mixed = mixed != 0;
-    if (c->N) GG_CUDA_TRY(cudaMemcpyAsync(c->in_rec.p, c->h_stage, c->N * sizeof(GGPart), cudaMemcpyHostToDevice,
+    if (c->N) GG_CUDA_TRY(cudaMemcpyAsync(c->in_rec.p, c->h_stage.p, c->N * sizeof(GGPart), cudaMemcpyHostToDevice,
                                           c->stream));
     GG_CUDA_TRY(cudaEventRecord(c->stage_ev, c->stream));
     return GG_OK;
@@ -990,17 +1081,9 @@ extern "C" gg_status gg_load_system_velocities(gg_ctx *c, const double *const *v
     if ((st = set_device(c))) return st;
     const long long N = c->N;
     if ((st = c->vel.ensure((size_t)3 * N + 3))) return st;
-    if ((size_t)N > c->h_vstage_cap) {
-        GG_CUDA_TRY(cudaEventSynchronize(c->vstage_ev));
-        if (c->h_vstage) cudaFreeHost(c->h_vstage);
-        c->h_vstage = nullptr;
-        c->h_vstage_cap = 0;
-        GG_CUDA_TRY(cudaMallocHost((void **)&c->h_vstage, (size_t)(N ? N : 1) * 3 * sizeof(double)));
-        c->h_vstage_cap = (size_t)(N ? N : 1);
-    }
-    GG_CUDA_TRY(cudaEventSynchronize(c->vstage_ev));
+    if ((st = c->h_vstage.ensure((size_t)N * 3, c->vstage_ev))) return st;
     const std::vector<HostChunk> ch = host_chunks(c);
-    double *dst = c->h_vstage;
+    double *dst = c->h_vstage.p;
 #pragma omp parallel for schedule(dynamic, 1)
     for (long long k = 0; k < (long long)ch.size(); k++) {
         const HostChunk q = ch[k];
@@ -1029,41 +1112,23 @@ extern "C" gg_status gg_evaluate_async(gg_ctx *c, const int32_t *active, int64_t
     if ((st = c->acc_d.ensure(outn * 3)) || (st = c->pot_d.ensure(outn))) return st;
     const int *d_active = nullptr;
     if (active) {
-        if ((size_t)n_active > c->h_active_cap) {
-            GG_CUDA_TRY(cudaEventSynchronize(c->act_ev));
-            if (c->h_active) cudaFreeHost(c->h_active);
-            c->h_active = nullptr;
-            c->h_active_cap = 0;
-            GG_CUDA_TRY(cudaMallocHost((void **)&c->h_active, (size_t)(n_active > 0 ? n_active : 1) * sizeof(int)));
-            c->h_active_cap = (size_t)(n_active > 0 ? n_active : 1);
-        }
-        GG_CUDA_TRY(cudaEventSynchronize(c->act_ev));
+        if ((st = c->h_active.ensure((size_t)n_active, c->act_ev))) return st;
         if ((st = c->active_d.ensure(n_active > 0 ? n_active : 1))) return st;
-        memcpy(c->h_active, active, (size_t)n_active * sizeof(int));
+        memcpy(c->h_active.p, active, (size_t)n_active * sizeof(int));
         if (n_active)
-            GG_CUDA_TRY(cudaMemcpyAsync(c->active_d.p, c->h_active, n_active * sizeof(int), cudaMemcpyHostToDevice, s));
+            GG_CUDA_TRY(cudaMemcpyAsync(c->active_d.p, c->h_active.p, n_active * sizeof(int), cudaMemcpyHostToDevice, s));
         GG_CUDA_TRY(cudaEventRecord(c->act_ev, s));
         d_active = c->active_d.p;
     }
     if ((st = run_walk(c, d_active, (int)n_active, nullptr, tol, theta, c->acc_d.p, c->pot_d.p, nullptr))) return st;
     if (flags) {
-        if ((size_t)nt > c->h_out_cap) {
-            GG_CUDA_TRY(cudaEventSynchronize(c->done_ev));
-            if (c->h_acc) cudaFreeHost(c->h_acc);
-            if (c->h_pot) cudaFreeHost(c->h_pot);
-            c->h_acc = c->h_pot = nullptr;
-            c->h_out_cap = 0;
-            const size_t cap = (size_t)(nt > 0 ? nt : 1);
-            GG_CUDA_TRY(cudaMallocHost((void **)&c->h_acc, cap * 3 * sizeof(double)));
-            GG_CUDA_TRY(cudaMallocHost((void **)&c->h_pot, cap * sizeof(double)));
-            c->h_out_cap = cap;
-        } else {
-            // the previous results may not have been fetched yet: they are overwritten in stream order
-        }
+        // unfetched results of an earlier call are overwritten in stream order
+        if ((flags & GG_ASYNC_COPY_ACC) && (st = c->h_acc.ensure((size_t)nt * 3, c->done_ev))) return st;
+        if ((flags & GG_ASYNC_COPY_POT) && (st = c->h_pot.ensure((size_t)nt, c->done_ev))) return st;
         if (nt && (flags & GG_ASYNC_COPY_ACC))
-            GG_CUDA_TRY(cudaMemcpyAsync(c->h_acc, c->acc_d.p, nt * 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+            GG_CUDA_TRY(cudaMemcpyAsync(c->h_acc.p, c->acc_d.p, nt * 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
         if (nt && (flags & GG_ASYNC_COPY_POT))
-            GG_CUDA_TRY(cudaMemcpyAsync(c->h_pot, c->pot_d.p, nt * sizeof(double), cudaMemcpyDeviceToHost, s));
+            GG_CUDA_TRY(cudaMemcpyAsync(c->h_pot.p, c->pot_d.p, nt * sizeof(double), cudaMemcpyDeviceToHost, s));
         c->async_n = nt;
         c->async_flags = flags;
     }
@@ -1081,6 +1146,20 @@ extern "C" gg_status gg_query(gg_ctx *c)
     return gg_cuda_fail(e);
 }
 
+// host copy spread over the OpenMP threads (results of large batches run to
+// hundreds of MB)
+static void parallel_copy(void *dst, const void *src, size_t bytes)
+{
+    const size_t chunk = (size_t)4 << 20;
+    const long long nchunks = (long long)((bytes + chunk - 1) / chunk);
+    if (nchunks <= 1) { memcpy(dst, src, bytes); return; }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long k = 0; k < nchunks; k++) {
+        const size_t off = (size_t)k * chunk, len = std::min(chunk, bytes - off);
+        memcpy((char *)dst + off, (const char *)src + off, len);
+    }
+}
+
 extern "C" gg_status gg_fetch_results(gg_ctx *c, double *acc_out, double *pot_out, gg_stats *stats)
 {
     if (!c) return GG_ERR_INVALID;
@@ -1090,13 +1169,51 @@ extern "C" gg_status gg_fetch_results(gg_ctx *c, double *acc_out, double *pot_ou
     const long long nt = c->async_n;
     if (acc_out) {
         if (!(c->async_flags & GG_ASYNC_COPY_ACC)) return GG_ERR_INVALID;
-        memcpy(acc_out, c->h_acc, (size_t)nt * 3 * sizeof(double));
+        parallel_copy(acc_out, c->h_acc.p, (size_t)nt * 3 * sizeof(double));
     }
     if (pot_out) {
         if (!(c->async_flags & GG_ASYNC_COPY_POT)) return GG_ERR_INVALID;
-        memcpy(pot_out, c->h_pot, (size_t)nt * sizeof(double));
+        parallel_copy(pot_out, c->h_pot.p, (size_t)nt * sizeof(double));
     }
+    // the evaluation and every transfer before it are done: hand the pinned
+    // buffers back for other contexts
+    c->h_stage.give_back(c->stage_ev);
+    c->h_vstage.give_back(c->vstage_ev);
+    c->h_active.give_back(c->act_ev);
+    c->h_acc.give_back(c->done_ev);
+    c->h_pot.give_back(c->done_ev);
+    c->async_flags = 0;
     st = collect_stats(c, stats);
     if (stats) stats->n_targets = nt;
+    return st;
+}
+
+// ---------------------------------------------------------------- device memory reservation
+extern "C" gg_status gg_reserve_device_pool(int32_t device, int64_t bytes)
+{
+    if (bytes < 0) return GG_ERR_INVALID;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return GG_ERR_INVALID;
+    }
+    GG_CUDA_TRY(cudaSetDevice(device));
+    keep_pool_memory(device);
+    cudaStream_t s;
+    GG_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    // grow the pool in 2 GB pieces, then give them all back to it
+    const size_t piece = (size_t)2 << 30;
+    std::vector<void *> got;
+    gg_status st = GG_OK;
+    for (int64_t left = bytes; left > 0; left -= (int64_t)piece) {
+        void *p = nullptr;
+        cudaError_t e = cudaMallocAsync(&p, std::min((size_t)left, piece), s);
+        if (e != cudaSuccess) { cudaGetLastError(); st = GG_ERR_NOMEM; break; }
+        got.push_back(p);
+    }
+    for (void *p : got) cudaFreeAsync(p, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    if (e != cudaSuccess && !st) st = gg_cuda_fail(e);
     return st;
 }

@@ -118,6 +118,7 @@ def load_library():
             "gg_load_velocities_device": (i32, [P, P]),
             "gg_drift": (i32, [P, dbl]),
             "gg_device_bytes": (i32, [P, ctypes.POINTER(i64)]),
+            "gg_reserve_device_pool": (i32, [i32, i64]),
             "gg_load_systems": (i32, [P, i32, P, P, P, P]),
             "gg_load_system_velocities": (i32, [P, P]),
             "gg_evaluate_async": (i32, [P, P, i64, dbl, dbl, i32]),
@@ -403,6 +404,11 @@ def direct_sum_fp64(d_pos, d_mass, d_h, n_src, d_targets, n_tgt, d_acc, d_pot, s
     lib = load_library()
     _check(lib.gg_direct_sum_fp64(n_src, _ptr(d_pos), _ptr(d_mass), _ptr(d_h), n_tgt, _ptr(d_targets), _ptr(d_acc),
                                   _ptr(d_pot), stream), "gg_direct_sum_fp64")
+
+
+def reserve_device_pool(nbytes, device=0):
+    """Grow the device's memory pool by nbytes once (see gg_reserve_device_pool)."""
+    _check(load_library().gg_reserve_device_pool(int(device), int(nbytes)), "gg_reserve_device_pool")
 
 
 def fp32_peak_tflops(stream=None):

@@ -23,9 +23,16 @@ served as a new solve of the drifted system (a "miss").
 The plain form (batching=False) serves one request at a time, one system per
 launch sequence, with the same library calls.
 
+Finished launches are fetched (results copied out of the library's pinned
+buffers by all host threads) by the scheduler itself; threaded=True hands the
+fetches to a completion thread instead, which helps only where the host has
+cores to spare for two concurrent OpenMP copies.
+
 The latency of a request is from its arrival to its result in host memory.
 """
 import collections
+import queue
+import threading
 import time
 
 import numpy as np
@@ -67,7 +74,8 @@ class _Context:
 
 class Server:
     def __init__(self, budget_bytes=120e9, tol=0.001, batching=True, max_batch_particles=8 << 20,
-                 max_batch_systems=1024, max_inflight=6, leaf=8, group=32, flush=64, device=0, tree_factory=None):
+                 max_batch_systems=1024, max_inflight=6, leaf=8, group=32, flush=64, device=0, tree_factory=None,
+                 threaded=False, reserve=False):
         self.budget = float(budget_bytes)
         self.tol = tol
         self.batching = batching
@@ -76,6 +84,9 @@ class Server:
         self.max_inflight = int(max_inflight) if batching else 1
         self.cfg = dict(leaf_size=leaf, group_size=group, flush=flush, device=device)
         self.tree_factory = tree_factory or ggb200.GravityTree
+        if reserve:
+            # map the whole budget once, before the first request
+            ggb200.reserve_device_pool(self.budget, device)
         self.pending_new = collections.deque()
         self.pending_re = collections.deque()
         self.resident = {}           # system id -> (_Context, index in context)
@@ -87,6 +98,10 @@ class Server:
         self.inflight = []           # (context, kind, [(request, k or None)])
         self.bytes_per_particle = 768.0   # predicted need, refined from gg_device_bytes
         self.fixed_bytes = 128 << 20      # walk stacks and other buffers independent of N
+        self.threaded = threaded
+        self._fetch_q, self._done_q = queue.Queue(), queue.Queue()
+        self._worker = None
+        self.fetching = 0            # launches finished on the device, results being copied out
         self.n_batches = 0
         self.evictions = 0
         self.peak_bytes = 0
@@ -203,33 +218,67 @@ class Server:
         self.inflight.append((c, "reeval", items))
         self.n_batches += 1
 
+    def _fetch_loop(self):
+        while True:
+            job = self._fetch_q.get()
+            if job is None:
+                return
+            c, kind, items = job
+            try:
+                res = c.tree.fetch()
+                self._done_q.put((c, kind, items, res, time.perf_counter()))
+            except Exception as e:   # handed to the scheduler thread
+                self._done_q.put((c, kind, items, e, time.perf_counter()))
+
     def poll(self, now):
         """Collect finished work (`now`: the caller's clock, for the LRU order);
         returns the number of requests completed."""
-        done = 0
         keep = []
         for c, kind, items in self.inflight:
             if not c.tree.query():
                 keep.append((c, kind, items))
-                continue
-            acc, pot, st = c.tree.fetch()
-            if st["error_word"]:
-                raise RuntimeError("device error word %d" % st["error_word"])
-            off = 0
-            for r, k in items:
-                n = r.n
-                r.acc, r.pot = acc[off:off + n].copy(), pot[off:off + n].copy()
-                off += n
-                r.t_done = time.perf_counter()
-                self.done.append(r)
-                done += 1
-            if kind == "new":
-                for k, sid in enumerate(c.sids):
-                    self.resident[sid] = (c, k)
-                    self.unsolved.discard(sid)
-            c.busy = False
-            c.last_use = now
+            elif self.threaded:
+                if self._worker is None:
+                    self._worker = threading.Thread(target=self._fetch_loop, daemon=True)
+                    self._worker.start()
+                self.fetching += 1
+                self._fetch_q.put((c, kind, items))
+            else:
+                res = c.tree.fetch()
+                self._done_q.put((c, kind, items, res, time.perf_counter()))
+                self.fetching += 1
         self.inflight = keep
+        done = 0
+        while True:
+            try:
+                c, kind, items, res, t_fetched = self._done_q.get_nowait()
+            except queue.Empty:
+                break
+            self.fetching -= 1
+            done += self._finish(c, kind, items, res, t_fetched, now)
+        return done
+
+    def _finish(self, c, kind, items, res, t_fetched, now):
+        if isinstance(res, Exception):
+            raise res
+        acc, pot, st = res
+        if st["error_word"]:
+            raise RuntimeError("device error word %d" % st["error_word"])
+        done = 0
+        off = 0
+        for r, k in items:
+            n = r.n
+            r.acc, r.pot = acc[off:off + n], pot[off:off + n]   # views of this launch's fresh arrays
+            off += n
+            r.t_done = t_fetched
+            self.done.append(r)
+            done += 1
+        if kind == "new":
+            for k, sid in enumerate(c.sids):
+                self.resident[sid] = (c, k)
+                self.unsolved.discard(sid)
+        c.busy = False
+        c.last_use = now
         return done
 
     def schedule(self, now):
@@ -288,9 +337,13 @@ class Server:
         return sid in self.unsolved
 
     def idle(self):
-        return not (self.pending_new or self.pending_re or self.inflight)
+        return not (self.pending_new or self.pending_re or self.inflight or self.fetching)
 
     def close(self):
+        if self._worker is not None:
+            self._fetch_q.put(None)
+            self._worker.join()
+            self._worker = None
         for c in self.contexts:
             c.tree.close()
         self.contexts = []
@@ -312,7 +365,7 @@ def run_trace(server, requests, realtime=True, poll_sleep=50e-6):
             i += 1
         server.poll(now)
         server.schedule(now)
-        if server.inflight and not server.pending_new and not server.pending_re:
+        if (server.inflight or server.fetching) and not server.pending_new and not server.pending_re:
             time.sleep(poll_sleep)
         elif not server.inflight and i < n:
             time.sleep(max(0.0, min(requests[i].arrival - (time.perf_counter() - t0), 1e-3)))

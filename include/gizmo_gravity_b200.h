@@ -136,6 +136,14 @@ gg_status gg_last_stats(gg_ctx *ctx, gg_stats *stats);
 /* device memory the context holds now (all its buffers), for callers that
  * admit work against a memory budget; no counterpart in the reference */
 gg_status gg_device_bytes(gg_ctx *ctx, int64_t *bytes);
+/* Contexts allocate their device buffers in stream order from the device's
+ * default memory pool, which this library sets to keep freed memory for
+ * reuse.  gg_reserve_device_pool grows that pool by `bytes` once (allocated
+ * and handed back at once), so that later contexts are served from memory
+ * already mapped: a server reserves its memory budget at start.  The memory
+ * stays with the process.  Returns GG_ERR_NOMEM if the device cannot hold it
+ * (what was reserved until then stays reserved).  Synchronous. */
+gg_status gg_reserve_device_pool(int32_t device, int64_t bytes);
 
 /* ---- drift of the resident tree ----------------------------------------
  * Re-evaluation between rebuilds, as GIZMO does when TreeReconstructFlag is

@@ -101,3 +101,11 @@ def test_small_budget_evicts_and_solves_misses_afresh():
         acc_d, _ = oracle.direct_sum(moved, s["mass"], s["h"])
         assert ics.error_stats(r.acc, acc_d)[1] < 2e-3
     srv.close()
+
+
+def test_device_pool_reservation():
+    import ggb200
+    ggb200.reserve_device_pool(1 << 30)      # maps 1 GB into this process's pool once
+    ggb200.reserve_device_pool(1 << 30)      # served from the pool the second time
+    with pytest.raises(ggb200.GravityError):
+        ggb200.reserve_device_pool(-1)
