@@ -14,8 +14,11 @@
 //   - relative pass: r^2 < (soft+0.6 len)^2 or
 //     r^2 < (maxsoft+0.6 len)^2, m len^2 > r^4 aold, or
 //     the target inside the 1.2*len box opens           (:2119-2147)
-// For a group of one target these are exactly the reference's tests.  Tests
-// run in FP64 on the FP64 centre of mass.  Used nodes and particles are
+// For a group of one target these are exactly the reference's tests, run in
+// FP64 on the FP64 centre of mass (exact mode).  Larger groups run the same
+// tests in FP32 on offsets from the group centre, with the box half-widths
+// rounded up; a test within FP32 rounding of its threshold may go either way,
+// which is far below the margin the group's conservative box adds.  Used nodes and particles are
 // appended (ballot + popc compaction) to per-warp shared-memory lists as
 // FP32 offsets from the group centre; a "far" list holds entries that are
 // Newtonian for every target of the group (no softening branch, no self
