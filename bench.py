@@ -551,6 +551,7 @@ def main():
     ap.add_argument("--group", type=int, default=32)
     ap.add_argument("--flush", type=int, default=64)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
+    ap.add_argument("--target-order", type=int, default=0, choices=[0, 1])
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--serve-window", type=float, default=2.0)
     args = ap.parse_args()
@@ -582,7 +583,8 @@ def main():
     d_pot = torch.empty(n, dtype=torch.float64, device=dev)
 
     tree = ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush,
-                              device=local, blocks_per_sm=args.blocks_per_sm)
+                              device=local, blocks_per_sm=args.blocks_per_sm,
+                              target_order=args.target_order)
     tree.set_stream(stream.cuda_stream)
     tree.load_device(d_rec, [n])
     # start-up Barnes-Hut pass gives OldAcc (accel.c:47-50), left on the device
@@ -632,7 +634,7 @@ def main():
 
     # stage breakdown on one extra instrumented step (outside the timed region)
     tprof = ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush, device=local,
-                               timing=True, blocks_per_sm=args.blocks_per_sm)
+                               timing=True, blocks_per_sm=args.blocks_per_sm, target_order=args.target_order)
     tprof.set_stream(stream.cuda_stream)
     tprof.load_device(d_rec, [n])
     tprof.build()
@@ -679,7 +681,8 @@ def main():
     if not args.no_e2e and rank == 0:
         old = np.linalg.norm(acc, axis=1)
         with ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush,
-                                device=local, blocks_per_sm=args.blocks_per_sm) as te:
+                                device=local, blocks_per_sm=args.blocks_per_sm,
+                              target_order=args.target_order) as te:
             def e2e_step():
                 te.load(ic["pos"], ic["mass"], ic["h"])
                 te.build()

@@ -89,30 +89,26 @@ struct Kahan {
 };
 
 // Cubic-spline softened force and potential factors for u = r/h < 1
-// (kernel.h:452-470).  The two pieces (u < 0.5 and 0.5 <= u < 1) are written
-// as one polynomial in u plus 1/u terms whose coefficients are selected by the
-// piece, so lanes on different pieces do not diverge:
-//   w_force = c0 + c1 u + c2 u^2 + c3 u^3 + c4 / u^3
-//   w_pot   = d0 + d1 / u + d2 u^2 + d3 u^3 + d4 u^4 + d5 u^5
-// iu = 1/u is passed in (the caller has it from r^-1 for free).  Returns
-// w_force, writes w_pot; they are still to be scaled by h^-3 and h^-1.
+// (kernel.h:452-470), without a branch or a per-piece coefficient choice.  The
+// outer piece (0.5 <= u < 1) equals the inner polynomial plus a correction
+// that vanishes below u = 0.5, written in t = max(u - 0.5, 0):
+//   w_force = 32/3 + u^2 (32 u - 38.4)  -  256 t^4 (t^2/6 + t/5 + 1/16) / u^3
+//   w_pot   = -2.8 + u^2 (16/3 + u^2 (6.4 u - 9.6))  +  t^5 (-6.4 - 128/15 t) / u
+// (the force correction is the mass the outer piece of the density removes,
+// divided by u^3; the potential correction integrates u times it from 0.5).
+// iu = 1/u is passed in (the caller has it from r^-1).  The corrections are
+// multiplied out starting from t, so a zero t stays zero however large iu is.
+// Returns w_force, writes w_pot; they are still to be scaled by h^-3 and h^-1.
 __device__ __forceinline__ float spline_wf(float u, float iu, float *wp)
 {
-    const bool in = u < 0.5f;
-    const float c0 = in ? 10.666666666667f : 21.333333333333f;
-    const float c1 = in ? 0.0f : -48.0f;
-    const float c2 = in ? -38.4f : 38.4f;
-    const float c3 = in ? 32.0f : -10.666666666667f;
-    const float c4 = in ? 0.0f : -0.066666666667f;
-    const float d0 = in ? -2.8f : -3.2f;
-    const float d1 = in ? 0.0f : 0.066666666667f;
-    const float d2 = in ? 5.333333333333f : 10.666666666667f;
-    const float d3 = in ? 0.0f : -16.0f;
-    const float d4 = in ? -9.6f : 9.6f;
-    const float d5 = in ? 6.4f : -2.133333333333f;
-    const float u2 = u * u, iu3 = iu * iu * iu;
-    *wp = fmaf(d1, iu, fmaf(u2, fmaf(u, fmaf(u, fmaf(u, d5, d4), d3), d2), d0));
-    return fmaf(c4, iu3, fmaf(u, fmaf(u, fmaf(u, c3, c2), c1), c0));
+    const float u2 = u * u;
+    const float t = fmaxf(u - 0.5f, 0.f);
+    const float t2 = t * t, t4 = t2 * t2;
+    const float fin = fmaf(u2, fmaf(u, 32.f, -38.4f), 10.666666666667f);
+    const float q = t4 * fmaf(t, fmaf(t, 0.166666666667f, 0.2f), 0.0625f);
+    const float pin = fmaf(u2, fmaf(u2, fmaf(u, 6.4f, -9.6f), 5.333333333333f), -2.8f);
+    *wp = fmaf((t4 * t) * fmaf(t, -8.533333333333f, -6.4f), iu, pin);
+    return fmaf(-256.f, ((q * iu) * iu) * iu, fin);
 }
 
 template <int TPL>
@@ -154,51 +150,56 @@ __device__ __forceinline__ void flush_far(const float4 *__restrict__ far, int nf
     __syncwarp();
 }
 
+// Near list: entries within the softening of some target of the group.  Most
+// of them need the spline for some lanes and the Newtonian form for others
+// (both for 85% of entries on the galaxy), so every lane evaluates both
+// branch-free and selects; without a branch the loop unrolls over entries and
+// independent entries overlap their dependency chains.  r^2 = 0 (the target
+// itself, or a coincident particle) contributes nothing and is not counted.
 template <int TPL>
 __device__ __forceinline__ void flush_near(const float4 *__restrict__ nearE, const float2 *__restrict__ nearH, int nn,
                                            Targets<TPL> &T)
 {
     __syncwarp();
     float px[TPL], py[TPL], pz[TPL], pp[TPL];
+    int self[TPL];
 #pragma unroll
-    for (int s = 0; s < TPL; s++) { px[s] = 0.f; py[s] = 0.f; pz[s] = 0.f; pp[s] = 0.f; T.nint[s] += nn; }
+    for (int s = 0; s < TPL; s++) { px[s] = 0.f; py[s] = 0.f; pz[s] = 0.f; pp[s] = 0.f; self[s] = 0; }
+#pragma unroll 2
     for (int j = 0; j < nn; j++) {
         const float4 e = nearE[j];
         const float2 hh = nearH[j];   // source kernel radius and its inverse
         const float hp = hh.x;
 #pragma unroll
         for (int s = 0; s < TPL; s++) {
-            float dx = e.x - T.x[s], dy = e.y - T.y[s], dz = e.z - T.z[s];
-            float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            if (r2 > 0.f) {
-                float hg = fmaxf(T.h[s], hp);
-                float rinv = rsqrtf(r2);
-                float fac, fpot;
-                if (r2 >= hg * hg) {
-                    float mr = e.w * rinv;
-                    fac = mr * rinv * rinv;
-                    fpot = -mr;
-                } else {
-                    float hinv = T.h[s] >= hp ? T.hinv[s] : hh.y;
-                    float u = r2 * rinv * hinv;
-                    float iu = hg * rinv;
-                    float wp;
-                    float wf = spline_wf(u, iu, &wp);
-                    fac = e.w * wf * hinv * hinv * hinv;
-                    fpot = e.w * wp * hinv;
-                }
-                px[s] = fmaf(dx, fac, px[s]);
-                py[s] = fmaf(dy, fac, py[s]);
-                pz[s] = fmaf(dz, fac, pz[s]);
-                pp[s] += fpot;
-            } else {
-                T.nint[s] -= 1;   // self (or a coincident particle): not an interaction
-            }
+            const float dx = e.x - T.x[s], dy = e.y - T.y[s], dz = e.z - T.z[s];
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const float hg = fmaxf(T.h[s], hp);
+            const float hinv = fminf(T.hinv[s], hh.y);   // 1/h_g: the inverses are rounded alike
+            const float rinv = rsqrtf(r2);
+            const float mr = e.w * rinv;
+            // spline for r < h_g (kernel.h:452-470), Newtonian beyond (:391-398)
+            const float u = r2 * rinv * hinv, iu = hg * rinv;
+            float wp;
+            const float wf = spline_wf(u, iu, &wp);
+            const float hinv2 = hinv * hinv;
+            const bool soft = r2 < hg * hg;
+            float fac = soft ? e.w * wf * (hinv2 * hinv) : mr * rinv * rinv;
+            float fpot = soft ? e.w * wp * hinv : -mr;
+            const bool use = r2 > 0.f;
+            fac = use ? fac : 0.f;
+            fpot = use ? fpot : 0.f;
+            self[s] += use ? 0 : 1;
+            px[s] = fmaf(dx, fac, px[s]);
+            py[s] = fmaf(dy, fac, py[s]);
+            pz[s] = fmaf(dz, fac, pz[s]);
+            pp[s] += fpot;
         }
     }
 #pragma unroll
     for (int s = 0; s < TPL; s++) {
         T.ax[s].add(px[s]); T.ay[s].add(py[s]); T.az[s].add(pz[s]); T.pot[s].add(pp[s]);
+        T.nint[s] += nn - self[s];
     }
     __syncwarp();
 }
