@@ -261,11 +261,12 @@ extern "C" void gg_config_default(gg_config *cfg)
 {
     memset(cfg, 0, sizeof *cfg);
     cfg->device = 0;
-    cfg->leaf_size = 16;   // measured best or tied on the galaxy, clustered and Plummer workloads
+    cfg->leaf_size = 8;
     cfg->group_size = 32;
     cfg->flush_threshold = 64;
     cfg->walk_blocks_per_sm = 0;
     cfg->timing = 0;
+    cfg->target_order = 1;
 }
 
 extern "C" const char *gg_strerror(gg_status s)
@@ -523,6 +524,9 @@ extern "C" gg_status gg_build(gg_ctx *c, const gg_domain *domains)
     GG_CUDA_TRY(cudaMemsetAsync(c->err.p, 0, 8 * sizeof(int), s));
     bool timing = c->cfg.timing != 0;
     if (timing) cudaEventRecord(c->ev[0], s);
+    // the extent pass also gives each system's range of kernel radii (used to
+    // order walk targets); explicit domains then replace its root cubes
+    if (N > 0) gg_launch_extent(c->in_rec.p, N, c->poff.p, S, c->extent_mm.p, c->hmm.p, c->dom.p, c->err.p, s);
     if (domains) {
         std::vector<GGDomainDev> d(S);
         for (int i = 0; i < S; i++) {
@@ -533,8 +537,6 @@ extern "C" gg_status gg_build(gg_ctx *c, const gg_domain *domains)
         }
         GG_CUDA_TRY(cudaMemcpyAsync(c->dom.p, d.data(), S * sizeof(GGDomainDev), cudaMemcpyHostToDevice, s));
         GG_CUDA_TRY(cudaStreamSynchronize(s));
-    } else if (N > 0) {
-        gg_launch_extent(c->in_rec.p, N, c->poff.p, S, c->extent_mm.p, c->hmm.p, c->dom.p, c->err.p, s);
     }
     if (N > 0) gg_launch_keys(c->in_rec.p, N, c->poff.p, S, c->dom.p, c->keys.p, c->perm.p, c->err.p, s);
     if (timing) cudaEventRecord(c->ev[1], s);
@@ -610,7 +612,8 @@ static gg_status run_walk(gg_ctx *c, const int *d_active, int n_active, const do
         if ((st = c->tkey.ensure(nt)) || (st = c->tval.ensure(nt)) || (st = c->tlist2.ensure(nt)) ||
             (st = c->tout2.ensure(nt)))
             return st;
-        st = gg_order_targets_by_softening(nt, tlist, tout, c->part.p, c->poff.p, S, c->tkey.p, c->tval.p,
+        st = gg_order_targets_by_softening(nt, tlist, tout, c->part.p, c->keys.p, c->poff.p, S, c->dom.p, c->hmm.p,
+                                           c->tkey.p, c->tval.p,
                                            c->tlist2.p, tout ? c->tout2.p : nullptr, c->sort_scratch.p, c->err.p, s);
         if (st) return st;
         tlist = c->tlist2.p;

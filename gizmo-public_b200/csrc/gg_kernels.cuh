@@ -68,8 +68,10 @@ void gg_launch_active(const int *active, int n_active, const unsigned *rank, int
 int gg_scan_scratch_ints();
 // targets reordered by (system, kernel radius), key order kept within a class
 gg_status gg_order_targets_by_softening(int nt, const int *tlist_in, const int *tout_in, const GGPart *parts,
-                                        const int *poff, int S, unsigned long long *key, unsigned *val,
-                                        int *tlist_out, int *tout_out, void *sort_scratch, int *err, cudaStream_t st);
+                                        const unsigned long long *pkeys, const int *poff, int S,
+                                        const GGDomainDev *dom, const unsigned *hmm, unsigned long long *key,
+                                        unsigned *val, int *tlist_out, int *tout_out, void *sort_scratch, int *err,
+                                        cudaStream_t st);
 
 void gg_launch_direct(long long n_src, const double *pos, const double *mass, const double *h, long long n_tgt,
                       const int *targets, double *acc, double *pot, cudaStream_t st);

@@ -1,5 +1,7 @@
 // gg_util.cu -- scans, walk-group tables, active-target compaction and the
 // FP64 direct summation used to measure force errors.
+#include <algorithm>
+
 #include "gg_internal.cuh"
 #include "gg_kernels.cuh"
 
@@ -304,22 +306,42 @@ extern "C" gg_status gg_fp32_peak_probe(double *tflops, void *stream)
     return GG_OK;
 }
 
-// ---- walk targets ordered by (system, softening) -------------------------------
-// Groups of targets that share a kernel radius keep the near field (entries
-// within the group's largest softening) as small as the targets need; in a
-// halo + disk system a group mixing the two would give its disk targets the
-// halo's larger near zone.  Within a class the targets stay in key order.
+// ---- walk targets ordered by (system, cell, softening class) ------------------
+// A walk group opens nodes for the largest softening among its targets, so in a
+// halo + disk system a group that mixes the two gives its disk targets the
+// halo's larger near zone.  Ordering the targets of a system by softening alone
+// keeps groups homogeneous but stretches the rarer class thin across dense
+// regions, and such groups then cost more than a warp's share of the whole
+// walk.  So the order is: Peano-Hilbert cell at the softening scale (the
+// deepest level whose cells are still as large as the system's largest kernel
+// radius, at most GG_ORDER_MAX_LEVEL), then softening class (quarter octaves of
+// h above the system's smallest), then key order.  Groups stay compact and are
+// homogeneous wherever a cell holds enough targets of one class.
+#define GG_ORDER_MAX_LEVEL 14
 __global__ void k_target_keys(int nt, const int *__restrict__ tlist, const GGPart *__restrict__ parts,
-                              const int *__restrict__ poff, int S, unsigned long long *key, unsigned *val)
+                              const unsigned long long *__restrict__ pkeys, const int *__restrict__ poff, int S,
+                              const GGDomainDev *__restrict__ dom, const unsigned *__restrict__ hmm, int lmax,
+                              unsigned long long *key, unsigned *val)
 {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
-        int pi = tlist ? tlist[t] : t;
+        const int pi = tlist ? tlist[t] : t;
         int lo = 0, hi = S - 1;
         while (lo < hi) {
             int mid = (lo + hi + 1) >> 1;
             if (__ldg(poff + mid) <= pi) lo = mid; else hi = mid - 1;
         }
-        key[t] = ((unsigned long long)lo << 32) | __float_as_uint(fmaxf(parts[pi].h, 0.f));
+        const unsigned hmin_bits = hmm[2 * lo];
+        const float hmax = __uint_as_float(hmm[2 * lo + 1]);
+        const double len = dom[lo].len;
+        int L = 0;
+        if (hmax > 0.f && isfinite(hmax))
+            while (L < lmax && ldexp(len, -(L + 1)) >= (double)hmax) L++;
+        else
+            L = lmax;
+        const unsigned long long cell = (pkeys[pi] >> (3 * (GG_MAX_LEVEL - L))) << (3 * (lmax - L));
+        const unsigned hb = __float_as_uint(fmaxf(parts[pi].h, 0.f));
+        const unsigned cls = hb > hmin_bits ? min((hb - hmin_bits) >> 21, 255u) : 0u;
+        key[t] = ((unsigned long long)lo << (3 * lmax + 8)) | (cell << 8) | cls;
         val[t] = (unsigned)t;
     }
 }
@@ -335,15 +357,18 @@ __global__ void k_target_apply(int nt, const unsigned *__restrict__ val, const i
 }
 
 gg_status gg_order_targets_by_softening(int nt, const int *tlist_in, const int *tout_in, const GGPart *parts,
-                                        const int *poff, int S, unsigned long long *key, unsigned *val,
-                                        int *tlist_out, int *tout_out, void *sort_scratch, int *err, cudaStream_t st)
+                                        const unsigned long long *pkeys, const int *poff, int S,
+                                        const GGDomainDev *dom, const unsigned *hmm, unsigned long long *key,
+                                        unsigned *val, int *tlist_out, int *tout_out, void *sort_scratch, int *err,
+                                        cudaStream_t st)
 {
     if (nt <= 0) return GG_OK;
     int sbits = 0;
     while ((1 << sbits) < S) sbits++;
-    int np = (32 + sbits + 7) / 8;
+    const int lmax = std::min(GG_ORDER_MAX_LEVEL, (64 - 8 - sbits) / 3);
+    const int np = (sbits + 3 * lmax + 8 + 7) / 8;
     int blocks = gg_num_sms() * 4;
-    k_target_keys<<<blocks, 256, 0, st>>>(nt, tlist_in, parts, poff, S, key, val);
+    k_target_keys<<<blocks, 256, 0, st>>>(nt, tlist_in, parts, pkeys, poff, S, dom, hmm, lmax, key, val);
     gg_note_launches(1);
     gg_status s = gg_sort_pairs_run(key, val, nt, np, 0, nullptr, 1, sort_scratch, err, st);
     if (s) return s;

@@ -167,7 +167,7 @@ def domain_to_dict(d):
 class GravityTree:
     """One library context: particles of one or more systems, their trees, walks."""
 
-    def __init__(self, leaf_size=16, group_size=32, flush=64, device=0, timing=False, blocks_per_sm=0, target_order=0):
+    def __init__(self, leaf_size=8, group_size=32, flush=64, device=0, timing=False, blocks_per_sm=0, target_order=1):
         lib = load_library()
         cfg = Config()
         lib.gg_config_default(ctypes.byref(cfg))

@@ -51,13 +51,15 @@ enum {
 
 typedef struct gg_config {
     int32_t device;           /* CUDA device ordinal */
-    int32_t leaf_size;        /* max particles per leaf bucket, 1..32 (default 16) */
+    int32_t leaf_size;        /* max particles per leaf bucket, 1..32 (default 8) */
     int32_t group_size;       /* targets per walk group, 1..64 (default 32) */
     int32_t flush_threshold;  /* interaction-list entries per flush, 32..128 (default 64) */
     int32_t walk_blocks_per_sm; /* persistent walk blocks per SM, 0 = default */
     int32_t timing;           /* 1: record per-stage device times into gg_stats */
-    int32_t target_order;     /* 0: walk groups follow key order (default); 1: when a system has
-                                 several kernel radii, groups gather targets of one radius */
+    int32_t target_order;     /* 1 (default): when a system holds several kernel radii, walk
+                                 targets are ordered by Peano-Hilbert cell at the softening
+                                 scale, then by radius, so groups are compact and of one radius
+                                 where they can be; 0: plain key order */
     int32_t reserved[1];
 } gg_config;
 
