@@ -101,7 +101,7 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- CPU baselines
-def cpu_reference_rate(ic, seconds=15.0, seed=1, tol=0.0025):
+def cpu_reference_rate(ic, seconds=15.0, seed=1, tol=0.0025, active_n=None):
     """Time the reference algorithm on the host cores on a bounded sample.
 
     Cost model of one step: tree build (serial in the reference) plus the walk
@@ -113,7 +113,7 @@ def cpu_reference_rate(ic, seconds=15.0, seed=1, tol=0.0025):
     try:
         import ref_runner
         if ref_runner.available():
-            return ref_runner.rate(ic, seconds=seconds, seed=seed, tol=tol)
+            return ref_runner.rate(ic, seconds=seconds, seed=seed, tol=tol, active_n=active_n)
     except ImportError:
         pass
     n = ic["pos"].shape[0]
@@ -157,8 +157,9 @@ def run_reference_arm(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref_runner
     if ref_runner.available():
+        active_n = int(round(args.active_frac * n)) if args.active_frac < 1.0 else None
         rates, info = ref_runner.steps_rate(ic, steps=args.steps, warmup=args.warmup, sample_n=args.ref_sample,
-                                            tol=args.tol)
+                                            tol=args.tol, active_n=active_n)
         v = float(np.mean(rates))
     else:
         vals = [cpu_reference_rate(ic, seconds=args.ref_seconds, seed=1000 + i, tol=args.tol)
@@ -554,6 +555,9 @@ def main():
     ap.add_argument("--target-order", type=int, default=1, choices=[0, 1])
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--serve-window", type=float, default=2.0)
+    # individual timesteps: the timed walk evaluates a seeded random fraction of
+    # the particles (the tree is still built over all of them)
+    ap.add_argument("--active-frac", type=float, default=1.0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -590,10 +594,22 @@ def main():
     # start-up Barnes-Hut pass gives OldAcc (accel.c:47-50), left on the device
     tree.build()
     tree.evaluate_device(d_acc, d_pot, err_tol_theta=0.7)
+    act, d_act, na = None, None, n
+    if args.active_frac < 1.0:
+        act = ics.random_active(n, args.active_frac, seed=multi.rank_seed(77, rank)).astype(np.int32)
+        na = int(act.size)
+        d_act = torch.from_numpy(act).to(dev)
+        # OldAcc of every particle from one relative pass over all of them
+        tree.build()
+        tree.evaluate_device(d_acc, d_pot, err_tol_force_acc=args.tol, err_tol_theta=0.0)
+
+    def walk(t):
+        t.evaluate_device(d_acc, d_pot, d_active=d_act, n_active=na if act is not None else 0,
+                          err_tol_force_acc=args.tol, err_tol_theta=0.0)
 
     def step():
         tree.build()
-        tree.evaluate_device(d_acc, d_pot, err_tol_force_acc=args.tol, err_tol_theta=0.0)
+        walk(tree)
 
     for _ in range(args.warmup):
         step()
@@ -614,7 +630,7 @@ def main():
     for k in range(args.steps):
         tree.build()
         ev[2 * k + 1].record(stream)
-        tree.evaluate_device(d_acc, d_pot, err_tol_force_acc=args.tol, err_tol_theta=0.0)
+        walk(tree)
         ev[2 * k + 2].record(stream)
     torch.cuda.synchronize()
     if dist:
@@ -626,7 +642,7 @@ def main():
     build_ms = (ev[0].elapsed_time(ev[1]) + sum(ev[2 * k].elapsed_time(ev[2 * k + 1])
                                                  for k in range(1, args.steps))) / args.steps
     total_ms = multi.max_over_ranks(dist, total_ms, device=dev)
-    n_all = multi.sum_over_ranks(dist, n, device=dev)
+    n_all = multi.sum_over_ranks(dist, na, device=dev)   # targets evaluated per step
     stats = tree.last_stats()
     ms_step = total_ms / args.steps
     value = n_all / (ms_step * 1e-3)
@@ -639,16 +655,20 @@ def main():
     tprof.load_device(d_rec, [n])
     tprof.build()
     tprof.evaluate_device(d_acc, d_pot, err_tol_theta=0.7)
+    if act is not None:
+        tprof.build()
+        tprof.evaluate_device(d_acc, d_pot, err_tol_force_acc=args.tol, err_tol_theta=0.0)
     tprof.build()
-    tprof.evaluate_device(d_acc, d_pot, err_tol_force_acc=args.tol, err_tol_theta=0.0)
+    walk(tprof)
     stages = tprof.last_stats()
     tprof.close()
 
     # force error against the FP64 direct sum on a seeded subsample
-    acc = d_acc.cpu().numpy()
-    pot = d_pot.cpu().numpy()
-    ne = min(args.err_targets, n)
-    tg = np.sort(np.random.default_rng(12345).choice(n, ne, replace=False)).astype(np.int32)
+    acc = d_acc[:na].cpu().numpy()
+    pot = d_pot[:na].cpu().numpy()
+    ne = min(args.err_targets, na)
+    rows = np.sort(np.random.default_rng(12345).choice(na, ne, replace=False))   # rows of the outputs
+    tg = (rows if act is None else act[rows]).astype(np.int32)                   # their particles
     dp = torch.from_numpy(ic["pos"]).to(dev)
     dm = torch.from_numpy(ic["mass"]).to(dev)
     dh = torch.from_numpy(ic["h"]).to(dev)
@@ -658,8 +678,8 @@ def main():
                            stream.cuda_stream)
     torch.cuda.synchronize()
     acc_dir, pot_dir = dacc.cpu().numpy(), dpot.cpu().numpy()
-    p50, p99, _ = ics.error_stats(acc[tg], acc_dir)
-    wsum = float(np.sum(ic["mass"][tg] * pot[tg]))
+    p50, p99, _ = ics.error_stats(acc[rows], acc_dir)
+    wsum = float(np.sum(ic["mass"][tg] * pot[rows]))
     wsum_dir = float(np.sum(ic["mass"][tg] * pot_dir))
     del dp, dm, dh, dacc, dpot
 
@@ -679,14 +699,21 @@ def main():
     # end to end through the public API with host buffers
     e2e = None
     if not args.no_e2e and rank == 0:
-        old = np.linalg.norm(acc, axis=1)
+        if act is None:
+            old = np.linalg.norm(acc, axis=1)
+        else:   # OldAcc of every particle: the device copy after one more full relative pass
+            tree.build()
+            tree.evaluate_device(d_acc, d_pot, err_tol_force_acc=args.tol, err_tol_theta=0.0)
+            old = torch.linalg.norm(d_acc, dim=1).cpu().numpy()
         with ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush,
                                 device=local, blocks_per_sm=args.blocks_per_sm,
                               target_order=args.target_order) as te:
+            out = (np.empty((na, 3)), np.empty(na))   # the caller's result arrays, reused every step
+
             def e2e_step():
                 te.load(ic["pos"], ic["mass"], ic["h"])
                 te.build()
-                return te.evaluate(old_acc=old, err_tol_force_acc=args.tol)
+                return te.evaluate(active=act, old_acc=old, err_tol_force_acc=args.tol, out=out)
             for _ in range(2):
                 e2e_step()
             t0 = time.perf_counter()
@@ -694,21 +721,23 @@ def main():
             for _ in range(ke):
                 e2e_step()
             dt = (time.perf_counter() - t0) / ke
-        e2e = {"value": n / dt, "unit": "particles/s", "h2d_bytes_per_step": int(n * (32 + 8)),
-               "d2h_bytes_per_step": int(n * (24 + 8)), "ms_per_step": dt * 1e3,
+        e2e = {"value": na / dt, "unit": "particles/s",
+               "h2d_bytes_per_step": int(n * (32 + 8) + (4 * na if act is not None else 0)),
+               "d2h_bytes_per_step": int(na * (24 + 8)), "ms_per_step": dt * 1e3,
                "path": "gg_load_particles (host FP64 arrays) + gg_build + gg_evaluate (host outputs, OldAcc in)"}
 
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
         ic_cpu = dict(ic)
         ic_cpu["acc_hint"] = acc
-        cpu = cpu_reference_rate(ic_cpu, seconds=args.cpu_seconds, tol=args.tol)
+        cpu = cpu_reference_rate(ic_cpu, seconds=args.cpu_seconds, tol=args.tol,
+                                 active_n=na if act is not None else None)
 
     out = {
         "metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": name, "n": n, "n_total": int(n_all), "err_tol_force_acc": args.tol,
+        "config": {"workload": name, "n": n, "active": na, "n_total": int(n_all), "err_tol_force_acc": args.tol,
                    "step": "extent+keys+sort+permute+tree+moments+relative walk (OldAcc on device)",
                    "l2": "inputs larger than L2 (32 B/particle records, 134 MB + tree)",
                    "leaf_size": args.leaf, "group_size": args.group, "flush": args.flush,
@@ -716,7 +745,7 @@ def main():
         "force_error": {"p50": p50, "p99": p99, "targets": ne, "vs": "FP64 direct sum (GPU, same pair rule)",
                         "pot_sum_rel_diff_sample": abs(wsum - wsum_dir) / abs(wsum_dir)},
         "interactions_per_step": inter, "interactions_per_s": inter / (ms_step * 1e-3),
-        "interactions_per_particle": inter / n,
+        "interactions_per_particle": inter / na,
         "stage_ms": {"keys": stages["ms_keys"], "sort": stages["ms_sort"], "build": stages["ms_build"],
                      "walk": stages["ms_walk"], "timed_build_phase": build_ms, "timed_walk_phase": walk_ms},
         "roofline": {"bound": "fp32", "kernel": "k_walk", "achieved": walk_tflops, "peak": peak32,

@@ -158,6 +158,20 @@ struct HostBuf {
     }
 };
 
+// host copy spread over the OpenMP threads (results of large batches run to
+// hundreds of MB)
+static void parallel_copy(void *dst, const void *src, size_t bytes)
+{
+    const size_t chunk = (size_t)4 << 20;
+    const long long nchunks = (long long)((bytes + chunk - 1) / chunk);
+    if (nchunks <= 1) { memcpy(dst, src, bytes); return; }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long k = 0; k < nchunks; k++) {
+        const size_t off = (size_t)k * chunk, len = std::min(chunk, bytes - off);
+        memcpy((char *)dst + off, (const char *)src + off, len);
+    }
+}
+
 struct gg_ctx {
     gg_config cfg;
     int device = 0;
@@ -223,8 +237,8 @@ struct gg_ctx {
     // for its own copy only
     cudaEvent_t stage_ev = nullptr, vstage_ev = nullptr;
     // asynchronous evaluation: staged active list, pinned results, completion
-    HostBuf<int> h_active;
-    HostBuf<double> h_acc, h_pot;
+    HostBuf<int> h_active, h_nint;
+    HostBuf<double> h_acc, h_pot, h_old;
     long long async_n = 0;
     int async_flags = 0;
     cudaEvent_t act_ev = nullptr, done_ev = nullptr;
@@ -358,6 +372,8 @@ extern "C" gg_status gg_destroy(gg_ctx *c)
     c->h_active.give_back(c->act_ev);
     c->h_acc.give_back(c->done_ev);
     c->h_pot.give_back(c->done_ev);
+    c->h_old.give_back(c->done_ev);
+    c->h_nint.give_back(c->done_ev);
     c->h_vstage.give_back(c->vstage_ev);
     c->h_stage.give_back(c->stage_ev);
     if (c->act_ev) cudaEventDestroy(c->act_ev);
@@ -722,33 +738,59 @@ extern "C" gg_status gg_evaluate(gg_ctx *c, const int32_t *active, int64_t n_act
     if (active && (n_active < 0 || n_active > c->N)) return GG_ERR_INVALID;
     size_t outn = (size_t)(c->N > 0 ? c->N : 1);
     if ((st = c->acc_d.ensure(outn * 3)) || (st = c->pot_d.ensure(outn)) || (st = c->nint_d.ensure(outn))) return st;
+    // host arrays go through pinned staging (copied in and out by all host
+    // threads): transfers from and to pageable memory run at a fraction of the
+    // link's speed
     const int *d_active = nullptr;
     if (active) {
         if ((st = c->active_d.ensure(n_active > 0 ? n_active : 1))) return st;
-        if (n_active)
-            GG_CUDA_TRY(cudaMemcpyAsync(c->active_d.p, active, n_active * sizeof(int), cudaMemcpyHostToDevice, s));
+        if (n_active) {
+            if ((st = c->h_active.ensure((size_t)n_active, c->act_ev))) return st;
+            parallel_copy(c->h_active.p, active, (size_t)n_active * sizeof(int));
+            GG_CUDA_TRY(cudaMemcpyAsync(c->active_d.p, c->h_active.p, n_active * sizeof(int), cudaMemcpyHostToDevice, s));
+            GG_CUDA_TRY(cudaEventRecord(c->act_ev, s));
+        }
         d_active = c->active_d.p;
     }
     if (old_acc) {
-        GG_CUDA_TRY(cudaMemcpyAsync(c->oldacc.p, old_acc, c->N * sizeof(double), cudaMemcpyHostToDevice, s));
+        if ((st = c->h_old.ensure((size_t)c->N, c->done_ev))) return st;
+        parallel_copy(c->h_old.p, old_acc, (size_t)c->N * sizeof(double));
+        GG_CUDA_TRY(cudaMemcpyAsync(c->oldacc.p, c->h_old.p, c->N * sizeof(double), cudaMemcpyHostToDevice, s));
         c->oldacc_valid = true;
     }
     if ((st = run_walk(c, d_active, (int)n_active, nullptr, tol, theta, c->acc_d.p, c->pot_d.p, c->nint_d.p)))
         return st;
     if (nt) {
-        GG_CUDA_TRY(cudaMemcpyAsync(acc_out, c->acc_d.p, nt * 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
-        if (pot_out) GG_CUDA_TRY(cudaMemcpyAsync(pot_out, c->pot_d.p, nt * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if ((st = c->h_acc.ensure((size_t)nt * 3, c->done_ev))) return st;
+        GG_CUDA_TRY(cudaMemcpyAsync(c->h_acc.p, c->acc_d.p, nt * 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (pot_out) {
+            if ((st = c->h_pot.ensure((size_t)nt, c->done_ev))) return st;
+            GG_CUDA_TRY(cudaMemcpyAsync(c->h_pot.p, c->pot_d.p, nt * sizeof(double), cudaMemcpyDeviceToHost, s));
+        }
+        if (ninter_out) {
+            if ((st = c->h_nint.ensure((size_t)nt, c->done_ev))) return st;
+            GG_CUDA_TRY(cudaMemcpyAsync(c->h_nint.p, c->nint_d.p, nt * sizeof(int), cudaMemcpyDeviceToHost, s));
+        }
     }
-    std::vector<int> ni;
-    if (ninter_out && nt) {
-        ni.resize(nt);
-        GG_CUDA_TRY(cudaMemcpyAsync(ni.data(), c->nint_d.p, nt * sizeof(int), cudaMemcpyDeviceToHost, s));
+    GG_CUDA_TRY(cudaEventRecord(c->done_ev, s));
+    st = collect_stats(c, stats);   // synchronises the stream
+    if (nt) {
+        parallel_copy(acc_out, c->h_acc.p, (size_t)nt * 3 * sizeof(double));
+        if (pot_out) parallel_copy(pot_out, c->h_pot.p, (size_t)nt * sizeof(double));
+        if (ninter_out) {
+            const int *ni = c->h_nint.p;
+#pragma omp parallel for schedule(static)
+            for (long long i = 0; i < nt; i++) ninter_out[i] = ni[i];
+        }
     }
-    st = collect_stats(c, stats);
-    c->h_stage.give_back(c->stage_ev);     // the loads before this evaluation are complete
+    // every transfer of this call and of the loads before it is complete
+    c->h_stage.give_back(c->stage_ev);
     c->h_vstage.give_back(c->vstage_ev);
-    if (ninter_out)
-        for (long long i = 0; i < nt; i++) ninter_out[i] = ni[i];
+    c->h_active.give_back(c->act_ev);
+    c->h_old.give_back(c->done_ev);
+    c->h_acc.give_back(c->done_ev);
+    c->h_pot.give_back(c->done_ev);
+    c->h_nint.give_back(c->done_ev);
     c->last.n_targets = nt;
     if (stats) stats->n_targets = nt;
     return st;
@@ -1147,20 +1189,6 @@ extern "C" gg_status gg_query(gg_ctx *c)
     if (e == cudaSuccess) return GG_OK;
     if (e == cudaErrorNotReady) { cudaGetLastError(); return GG_PENDING; }
     return gg_cuda_fail(e);
-}
-
-// host copy spread over the OpenMP threads (results of large batches run to
-// hundreds of MB)
-static void parallel_copy(void *dst, const void *src, size_t bytes)
-{
-    const size_t chunk = (size_t)4 << 20;
-    const long long nchunks = (long long)((bytes + chunk - 1) / chunk);
-    if (nchunks <= 1) { memcpy(dst, src, bytes); return; }
-#pragma omp parallel for schedule(dynamic, 1)
-    for (long long k = 0; k < nchunks; k++) {
-        const size_t off = (size_t)k * chunk, len = std::min(chunk, bytes - off);
-        memcpy((char *)dst + off, (const char *)src + off, len);
-    }
 }
 
 extern "C" gg_status gg_fetch_results(gg_ctx *c, double *acc_out, double *pot_out, gg_stats *stats)

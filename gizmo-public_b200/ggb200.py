@@ -237,14 +237,21 @@ class GravityTree:
         _check(self._lib.gg_get_domains(self._h, arr), "gg_get_domains")
         return [domain_to_dict(d) for d in arr]
 
-    def evaluate(self, active=None, old_acc=None, err_tol_force_acc=0.0025, err_tol_theta=0.0, want_ninter=False):
-        """Walk the trees for `active` particles (None = all).  Returns (acc, pot, ninter|None, stats)."""
+    def evaluate(self, active=None, old_acc=None, err_tol_force_acc=0.0025, err_tol_theta=0.0, want_ninter=False,
+                 out=None):
+        """Walk the trees for `active` particles (None = all).  Returns (acc, pot, ninter|None, stats).
+        out: optional (acc (n,3), pot (n)) float64 arrays to write into, reused across calls."""
         act = None
         if active is not None:
             act = np.ascontiguousarray(active, dtype=np.int32)
         nt = self.n if act is None else act.shape[0]
-        acc = np.empty((nt, 3), dtype=np.float64)
-        pot = np.empty(nt, dtype=np.float64)
+        if out is not None:
+            acc, pot = out
+            assert acc.shape == (nt, 3) and pot.shape == (nt,) and acc.dtype == np.float64 and pot.dtype == np.float64
+            assert acc.flags.c_contiguous and pot.flags.c_contiguous
+        else:
+            acc = np.empty((nt, 3), dtype=np.float64)
+            pot = np.empty(nt, dtype=np.float64)
         nint = np.empty(nt, dtype=np.int64) if want_ninter else None
         oa = None if old_acc is None else np.ascontiguousarray(old_acc, dtype=np.float64)
         st = Stats()

@@ -228,7 +228,7 @@ def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeou
             shutil.rmtree(d, ignore_errors=True)
 
 
-def steps_rate(ic, steps=3, warmup=1, sample_n=16384, seed=1, tol=0.0025, threads=None):
+def steps_rate(ic, steps=3, warmup=1, sample_n=16384, seed=1, tol=0.0025, threads=None, active_n=None):
     """The reference's particles/s per steady-state step, from a bounded sample.
 
     One run of GIZMO's own code: start-up passes on a seeded random sample of
@@ -241,27 +241,29 @@ def steps_rate(ic, steps=3, warmup=1, sample_n=16384, seed=1, tol=0.0025, thread
     ns = min(n, sample_n)
     sample = np.sort(np.random.default_rng(seed).choice(n, ns, replace=False))
     res = run(ic, tol=tol, steps=warmup + steps, sample=sample, threads=cores, sample_only=True)
+    n_eval = n if active_n is None else int(active_n)   # targets a step evaluates
     rates, per_list = [], []
     for st in res["info"]["steps"][warmup:]:
         per = max(st["t_gravity"] - st["t_build"], 1e-12) / ns
-        rates.append(n / (st["t_domain"] + st["t_build"] + per * n))
+        rates.append(n_eval / (st["t_domain"] + st["t_build"] + per * n_eval))
         per_list.append(per)
     last = res["info"]["steps"][-1]
     info = {"unit": "particles/s", "cores": cores, "kind": "reference",
             "sample": "GIZMO's own domain_Decomposition + tree build + relative gravity walk (compiled reference, "
                       "FP64, OpenMP %d threads) with %d seeded random active targets of %d; walk time per target "
-                      "scaled to all targets" % (cores, ns, n),
+                      "scaled to the %d targets of a step" % (cores, ns, n, n_eval),
             "t_domain_s": last["t_domain"], "t_build_s": last["t_build"],
             "t_walk_per_particle_us": float(np.mean(per_list)) * 1e6}
     return rates, info
 
 
-def rate(ic, seconds=15.0, seed=1, tol=0.0025, threads=None):
+def rate(ic, seconds=15.0, seed=1, tol=0.0025, threads=None, active_n=None):
     """One bounded measurement of the reference's step rate (about `seconds` of walk)."""
     n = ic["pos"].shape[0]
     probe, pinfo = steps_rate(ic, steps=1, warmup=0, sample_n=512, seed=seed, tol=tol, threads=threads)
     per = pinfo["t_walk_per_particle_us"] * 1e-6
     ns = int(min(n, max(512, seconds / max(per, 1e-9))))
-    rates, info = steps_rate(ic, steps=1, warmup=0, sample_n=ns, seed=seed + 1, tol=tol, threads=threads)
+    rates, info = steps_rate(ic, steps=1, warmup=0, sample_n=ns, seed=seed + 1, tol=tol, threads=threads,
+                             active_n=active_n)
     info["value"] = float(np.mean(rates))
     return info
