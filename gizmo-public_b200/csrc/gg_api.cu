@@ -214,6 +214,9 @@ struct gg_ctx {
     DevBuf<double> dts;
     HostBuf<double> h_vstage;
     DevBuf<double> oldacc_save;           // autotuner: every trial starts from the same OldAcc
+    DevBuf<int4> e_chunks;                // energy checks: chunk descriptors, partials, results
+    DevBuf<int> e_first;
+    DevBuf<double> e_part, e_out;
     bool oldacc_valid = false;
     DevBuf<GGGroup> groups;
     DevBuf<int> ngroups, gscan, toff, flag, flagscan, tlist, tout, scan_scratch, active_d;
@@ -252,6 +255,7 @@ struct gg_ctx {
         f(t_start); f(t_end); f(t_level); f(t_parent); f(t_sys); f(t_nch); f(t_child); f(t_counter); f(t_bnd);
         f(t_depth); f(t_nnodes); f(t_bsum); f(t_boff); f(t_mass64); f(nodes);
         f(oldacc); f(vel); f(kin); f(kin_counter); f(dts); f(oldacc_save);
+        f(e_chunks); f(e_first); f(e_part); f(e_out);
         f(groups); f(ngroups); f(gscan); f(toff); f(flag); f(flagscan); f(tlist); f(tout); f(scan_scratch);
         f(active_d); f(counters); f(inter); f(stack); f(err); f(acc_d); f(pot_d); f(nint_d);
     }
@@ -603,9 +607,10 @@ static gg_status walk_setup(gg_ctx *c)
     return GG_OK;
 }
 
-// run the walk; outputs to device pointers
+// run the walk; outputs to device pointers.  pot_only: the potential-only
+// walk (no acceleration output, OldAcc left as it is)
 static gg_status run_walk(gg_ctx *c, const int *d_active, int n_active, const double *d_old_acc, double tol,
-                          double theta, double *d_acc, double *d_pot, int *d_nint)
+                          double theta, double *d_acc, double *d_pot, int *d_nint, bool pot_only = false)
 {
     gg_status st;
     cudaStream_t s = c->stream;
@@ -651,7 +656,7 @@ static gg_status run_walk(gg_ctx *c, const int *d_active, int n_active, const do
     p.tout = tout;
     p.perm = c->perm.p;
     p.oldacc_in = c->oldacc_valid ? c->oldacc.p : nullptr;
-    p.oldacc_out = c->oldacc.p;
+    p.oldacc_out = pot_only ? nullptr : c->oldacc.p;
     p.tol = tol;
     p.theta = theta;
     p.acc = d_acc;
@@ -664,11 +669,13 @@ static gg_status run_walk(gg_ctx *c, const int *d_active, int n_active, const do
     p.err = c->err.p;
     p.group_size = c->cfg.group_size;
     p.flush = c->cfg.flush_threshold;
+    p.pot_only = pot_only ? 1 : 0;
+    if (pot_only) p.acc = nullptr;
     int tpl = c->cfg.group_size > 32 ? 2 : 1;
     if (c->cfg.timing) cudaEventRecord(c->ev[4], s);
     gg_launch_walk(p, tpl, c->walk_blocks, s);
     if (c->cfg.timing) cudaEventRecord(c->ev[5], s);
-    c->oldacc_valid = true;
+    if (!pot_only) c->oldacc_valid = true;
     GG_CUDA_TRY(cudaGetLastError());
     return GG_OK;
 }
@@ -1247,4 +1254,93 @@ extern "C" gg_status gg_reserve_device_pool(int32_t device, int64_t bytes)
     cudaStreamDestroy(s);
     if (e != cudaSuccess && !st) st = gg_cuda_fail(e);
     return st;
+}
+
+// ---------------------------------------------------------------- potential-only walk
+extern "C" gg_status gg_evaluate_potential_device(gg_ctx *c, const int32_t *d_active, int64_t n_active,
+                                                  const double *d_old_acc, double tol, double theta, double *d_pot)
+{
+    if (!c || !d_pot) return GG_ERR_INVALID;
+    if (!c->built) return GG_ERR_NOT_BUILT;
+    if (d_active && (n_active < 0 || n_active > c->N)) return GG_ERR_INVALID;
+    if (tol < 0 || theta < 0) return GG_ERR_INVALID;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    return run_walk(c, d_active, (int)n_active, d_old_acc, tol, theta, nullptr, d_pot, nullptr, true);
+}
+
+extern "C" gg_status gg_evaluate_potential(gg_ctx *c, const int32_t *active, int64_t n_active, const double *old_acc,
+                                           double tol, double theta, double *pot_out, gg_stats *stats)
+{
+    if (!c || !pot_out) return GG_ERR_INVALID;
+    if (!c->built) return GG_ERR_NOT_BUILT;
+    if (tol < 0 || theta < 0) return GG_ERR_INVALID;
+    if (active && (n_active < 0 || n_active > c->N)) return GG_ERR_INVALID;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    cudaStream_t s = c->stream;
+    const long long nt = active ? n_active : c->N;
+    if ((st = c->pot_d.ensure((size_t)(c->N > 0 ? c->N : 1)))) return st;
+    const int *d_active = nullptr;
+    if (active) {
+        if ((st = c->active_d.ensure(n_active > 0 ? n_active : 1))) return st;
+        if (n_active) {
+            if ((st = c->h_active.ensure((size_t)n_active, c->act_ev))) return st;
+            parallel_copy(c->h_active.p, active, (size_t)n_active * sizeof(int));
+            GG_CUDA_TRY(cudaMemcpyAsync(c->active_d.p, c->h_active.p, n_active * sizeof(int), cudaMemcpyHostToDevice, s));
+            GG_CUDA_TRY(cudaEventRecord(c->act_ev, s));
+        }
+        d_active = c->active_d.p;
+    }
+    if (old_acc) {   // becomes the context's OldAcc, as in gg_evaluate
+        if ((st = c->h_old.ensure((size_t)c->N, c->done_ev))) return st;
+        parallel_copy(c->h_old.p, old_acc, (size_t)c->N * sizeof(double));
+        GG_CUDA_TRY(cudaMemcpyAsync(c->oldacc.p, c->h_old.p, c->N * sizeof(double), cudaMemcpyHostToDevice, s));
+        c->oldacc_valid = true;
+    }
+    st = run_walk(c, d_active, (int)n_active, nullptr, tol, theta, nullptr, c->pot_d.p, nullptr, true);
+    if (st) return st;
+    if (nt) {
+        if ((st = c->h_pot.ensure((size_t)nt, c->done_ev))) return st;
+        GG_CUDA_TRY(cudaMemcpyAsync(c->h_pot.p, c->pot_d.p, nt * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    GG_CUDA_TRY(cudaEventRecord(c->done_ev, s));
+    st = collect_stats(c, stats);
+    if (nt) parallel_copy(pot_out, c->h_pot.p, (size_t)nt * sizeof(double));
+    c->h_active.give_back(c->act_ev);
+    c->h_old.give_back(c->done_ev);
+    c->h_pot.give_back(c->done_ev);
+    c->last.n_targets = nt;
+    if (stats) stats->n_targets = nt;
+    return st;
+}
+
+// ---------------------------------------------------------------- energy and momentum checks
+extern "C" gg_status gg_energy_device(gg_ctx *c, const double *d_acc, const double *d_pot, double *out)
+{
+    if (!c || !out || c->S < 1) return GG_ERR_INVALID;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    const int S = c->S;
+    const long long chunk = 65536;
+    std::vector<int4> ch;
+    std::vector<int> first(S + 1);
+    for (int s = 0; s < S; s++) {
+        first[s] = (int)ch.size();
+        for (long long b = c->h_poff[s]; b < c->h_poff[s + 1]; b += chunk)
+            ch.push_back(make_int4(s, (int)b, (int)std::min<long long>(b + chunk, c->h_poff[s + 1]), 0));
+    }
+    first[S] = (int)ch.size();
+    const size_t nc = ch.size();
+    if ((st = c->e_chunks.ensure(nc + 1)) || (st = c->e_first.ensure(S + 1)) || (st = c->e_part.ensure(4 * nc + 4)) ||
+        (st = c->e_out.ensure(4 * (size_t)S)))
+        return st;
+    cudaStream_t s = c->stream;
+    if (nc) GG_CUDA_TRY(cudaMemcpyAsync(c->e_chunks.p, ch.data(), nc * sizeof(int4), cudaMemcpyHostToDevice, s));
+    GG_CUDA_TRY(cudaMemcpyAsync(c->e_first.p, first.data(), (S + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
+    gg_launch_energy(c->e_chunks.p, (int)nc, c->e_first.p, S, c->in_rec.p, d_acc, d_pot, c->e_part.p, c->e_out.p, s);
+    GG_CUDA_TRY(cudaGetLastError());
+    GG_CUDA_TRY(cudaMemcpyAsync(out, c->e_out.p, 4 * (size_t)S * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GG_CUDA_TRY(cudaStreamSynchronize(s));
+    return GG_OK;
 }

@@ -52,6 +52,7 @@ struct WalkParams {
     int *err;
     int group_size;
     int flush;
+    int pot_only;               // potential-only walk: acc and oldacc_out unused, pot required
 };
 int gg_walk_smem_bytes(int flush, int tpl);
 void gg_launch_walk(const WalkParams &p, int tpl, int blocks_per_sm, cudaStream_t st);
@@ -82,3 +83,7 @@ void gg_launch_node_kinematics(const GGPart *parts, const unsigned *perm, const 
 void gg_launch_drift(GGPart *in_rec, GGPart *parts, const unsigned *perm, const double *vel, const int *poff, int S,
                      const double *dts, double dt_all, GGNode *nodes, const double4 *kin, const int *node_sys, const int *nnodes,
                      int n, int ncap, cudaStream_t st);
+
+// FP64 per-system sums {1/2 sum m phi, sum m a} (gg_util.cu)
+void gg_launch_energy(const int4 *chunks, int nchunks, const int *sys_first_chunk, int S, const GGPart *rec,
+                      const double *acc, const double *pot, double *part, double *out, cudaStream_t st);

@@ -376,3 +376,54 @@ gg_status gg_order_targets_by_softening(int nt, const int *tlist_in, const int *
     gg_note_launches(1);
     return GG_OK;
 }
+
+// ---- FP64 energy and momentum checks (global.c:54 potential energy) ----------
+// One block per chunk of one system sums m*phi/2 and m*a over its particles
+// (load order) in a fixed order; a second kernel adds each system's chunk
+// partials in chunk order, so the result does not depend on scheduling.
+__global__ void k_energy_chunks(const int4 *__restrict__ chunks, const GGPart *__restrict__ rec,
+                                const double *__restrict__ acc, const double *__restrict__ pot, double *part)
+{
+    const int4 ch = chunks[blockIdx.x];   // {system, first, end, unused}
+    double w = 0.0, fx = 0.0, fy = 0.0, fz = 0.0;
+    for (int i = ch.y + (int)threadIdx.x; i < ch.z; i += blockDim.x) {
+        const double m = (double)rec[i].m;
+        if (pot) w += 0.5 * m * pot[i];
+        if (acc) {
+            fx += m * acc[3 * (size_t)i];
+            fy += m * acc[3 * (size_t)i + 1];
+            fz += m * acc[3 * (size_t)i + 2];
+        }
+    }
+    __shared__ double sh[4][256];
+    sh[0][threadIdx.x] = w; sh[1][threadIdx.x] = fx; sh[2][threadIdx.x] = fy; sh[3][threadIdx.x] = fz;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o)
+            for (int q = 0; q < 4; q++) sh[q][threadIdx.x] += sh[q][threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) part[4 * (size_t)blockIdx.x + threadIdx.x] = sh[threadIdx.x][0];
+}
+
+__global__ void k_energy_systems(const int *__restrict__ sys_first_chunk, int S, const double *__restrict__ part,
+                                 double *out)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int c = sys_first_chunk[s]; c < sys_first_chunk[s + 1]; c++)
+        for (int q = 0; q < 4; q++) v[q] += part[4 * (size_t)c + q];
+    for (int q = 0; q < 4; q++) out[4 * (size_t)s + q] = v[q];
+}
+
+void gg_launch_energy(const int4 *chunks, int nchunks, const int *sys_first_chunk, int S, const GGPart *rec,
+                      const double *acc, const double *pot, double *part, double *out, cudaStream_t st)
+{
+    if (nchunks > 0) {
+        k_energy_chunks<<<nchunks, 256, 0, st>>>(chunks, rec, acc, pot, part);
+        gg_note_launches(1);
+    }
+    k_energy_systems<<<(S + 127) / 128, 128, 0, st>>>(sys_first_chunk, S, part, out);
+    gg_note_launches(1);
+}

@@ -119,7 +119,8 @@ struct Targets {
     int nint[TPL];
 };
 
-template <int TPL>
+// POT: the potential-only walk (force_treeevaluate_potential, forcetree.c:3169-3474)
+template <int TPL, bool POT>
 __device__ __forceinline__ void flush_far(const float4 *__restrict__ far, int nf, Targets<TPL> &T)
 {
     __syncwarp();
@@ -135,16 +136,19 @@ __device__ __forceinline__ void flush_far(const float4 *__restrict__ far, int nf
             float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             float rinv = rsqrtf(r2);
             float mr = e.w * rinv;
-            float fac = mr * rinv * rinv;
-            px[s] = fmaf(dx, fac, px[s]);
-            py[s] = fmaf(dy, fac, py[s]);
-            pz[s] = fmaf(dz, fac, pz[s]);
+            if (!POT) {
+                float fac = mr * rinv * rinv;
+                px[s] = fmaf(dx, fac, px[s]);
+                py[s] = fmaf(dy, fac, py[s]);
+                pz[s] = fmaf(dz, fac, pz[s]);
+            }
             pp[s] -= mr;
         }
     }
 #pragma unroll
     for (int s = 0; s < TPL; s++) {
-        T.ax[s].add(px[s]); T.ay[s].add(py[s]); T.az[s].add(pz[s]); T.pot[s].add(pp[s]);
+        if (!POT) { T.ax[s].add(px[s]); T.ay[s].add(py[s]); T.az[s].add(pz[s]); }
+        T.pot[s].add(pp[s]);
         T.nint[s] += nf;
     }
     __syncwarp();
@@ -156,7 +160,9 @@ __device__ __forceinline__ void flush_far(const float4 *__restrict__ far, int nf
 // branch-free and selects; without a branch the loop unrolls over entries and
 // independent entries overlap their dependency chains.  r^2 = 0 (the target
 // itself, or a coincident particle) contributes nothing and is not counted.
-template <int TPL>
+// POT: the potential-only walk, which has no r^2 > 0 condition: an r = 0 pair
+// adds m w_pot(0) / h like any other (the caller removes the self term).
+template <int TPL, bool POT>
 __device__ __forceinline__ void flush_near(const float4 *__restrict__ nearE, const float2 *__restrict__ nearH, int nn,
                                            Targets<TPL> &T)
 {
@@ -176,7 +182,7 @@ __device__ __forceinline__ void flush_near(const float4 *__restrict__ nearE, con
             const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             const float hg = fmaxf(T.h[s], hp);
             const float hinv = fminf(T.hinv[s], hh.y);   // 1/h_g: the inverses are rounded alike
-            const float rinv = rsqrtf(r2);
+            const float rinv = rsqrtf(POT ? fmaxf(r2, 1e-30f) : r2);   // finite at r = 0 when it counts
             const float mr = e.w * rinv;
             // spline for r < h_g (kernel.h:452-470), Newtonian beyond (:391-398)
             const float u = r2 * rinv * hinv, iu = hg * rinv;
@@ -184,21 +190,26 @@ __device__ __forceinline__ void flush_near(const float4 *__restrict__ nearE, con
             const float wf = spline_wf(u, iu, &wp);
             const float hinv2 = hinv * hinv;
             const bool soft = r2 < hg * hg;
-            float fac = soft ? e.w * wf * (hinv2 * hinv) : mr * rinv * rinv;
             float fpot = soft ? e.w * wp * hinv : -mr;
-            const bool use = r2 > 0.f;
-            fac = use ? fac : 0.f;
-            fpot = use ? fpot : 0.f;
-            self[s] += use ? 0 : 1;
-            px[s] = fmaf(dx, fac, px[s]);
-            py[s] = fmaf(dy, fac, py[s]);
-            pz[s] = fmaf(dz, fac, pz[s]);
-            pp[s] += fpot;
+            if (POT) {
+                pp[s] += fpot;
+            } else {
+                float fac = soft ? e.w * wf * (hinv2 * hinv) : mr * rinv * rinv;
+                const bool use = r2 > 0.f;
+                fac = use ? fac : 0.f;
+                fpot = use ? fpot : 0.f;
+                self[s] += use ? 0 : 1;
+                px[s] = fmaf(dx, fac, px[s]);
+                py[s] = fmaf(dy, fac, py[s]);
+                pz[s] = fmaf(dz, fac, pz[s]);
+                pp[s] += fpot;
+            }
         }
     }
 #pragma unroll
     for (int s = 0; s < TPL; s++) {
-        T.ax[s].add(px[s]); T.ay[s].add(py[s]); T.az[s].add(pz[s]); T.pot[s].add(pp[s]);
+        if (!POT) { T.ax[s].add(px[s]); T.ay[s].add(py[s]); T.az[s].add(pz[s]); }
+        T.pot[s].add(pp[s]);
         T.nint[s] += nn - self[s];
     }
     __syncwarp();
@@ -231,7 +242,7 @@ __device__ __forceinline__ int warp_incl_scan(int v, int lane)
 // F64T: opening tests in FP64 (used for one-target groups, where the tests are
 // exactly the reference's); otherwise the tests run in FP32 on FP64-formed
 // offsets from the group centre, against a bounding box rounded outwards.
-template <int TPL, int MINB, bool F64T>
+template <int TPL, int MINB, bool F64T, bool POT>
 __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
 {
     extern __shared__ float4 walk_smem[];
@@ -460,8 +471,8 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
             const int next_k = pop_nodes(next_node);
             GGNode nxt;
             if (lane < next_k) nxt = load_node(p.nodes + next_node);
-            if (nf >= FL) { flush_far<TPL>(far, nf, T); nf = 0; }
-            if (nn >= FL) { flush_near<TPL>(nearE, nearH, nn, T); nn = 0; }
+            if (nf >= FL) { flush_far<TPL, POT>(far, nf, T); nf = 0; }
+            if (nn >= FL) { flush_near<TPL, POT>(nearE, nearH, nn, T); nn = 0; }
             // opened leaves -> particles, 32 at a time
             {
                 int cnt = (act == 3) ? -nb : 0;
@@ -511,8 +522,8 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
                     nn += __popc(mn);
                     list_far += __popc(mf);
                     list_near += __popc(mn);
-                    if (nf >= FL) { flush_far<TPL>(far, nf, T); nf = 0; }
-                    if (nn >= FL) { flush_near<TPL>(nearE, nearH, nn, T); nn = 0; }
+                    if (nf >= FL) { flush_far<TPL, POT>(far, nf, T); nf = 0; }
+                    if (nn >= FL) { flush_near<TPL, POT>(nearE, nearH, nn, T); nn = 0; }
                 }
             }
             k = next_k;
@@ -523,8 +534,8 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
             if (lane == 0) atomicOr(p.err, GG_EBIT_STACK_OVERFLOW);
             continue;
         }
-        if (nf > 0) flush_far<TPL>(far, nf, T);
-        if (nn > 0) flush_near<TPL>(nearE, nearH, nn, T);
+        if (nf > 0) flush_far<TPL, POT>(far, nf, T);
+        if (nn > 0) flush_near<TPL, POT>(nearE, nearH, nn, T);
 
         // ---- results
         int mycount = 0;
@@ -535,13 +546,20 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
             int pi = tpi[s];
             unsigned li = p.perm[pi];
             int o = p.tout ? p.tout[t] : (int)li;
-            double ax = T.ax[s].value(), ay = T.ay[s].value(), az = T.az[s].value();
-            p.acc[3 * (size_t)o] = ax;
-            p.acc[3 * (size_t)o + 1] = ay;
-            p.acc[3 * (size_t)o + 2] = az;
-            if (p.pot) p.pot[o] = T.pot[s].value();
+            if (POT) {
+                // compute_potential removes the self term m_i kernel(0) / h_i
+                // (potential.c:137-145); subtract the FP32 value the walk added
+                const float mi = p.parts[pi].m;
+                p.pot[o] = T.pot[s].value() - (double)((mi * -2.8f) * T.hinv[s]);
+            } else {
+                double ax = T.ax[s].value(), ay = T.ay[s].value(), az = T.az[s].value();
+                p.acc[3 * (size_t)o] = ax;
+                p.acc[3 * (size_t)o + 1] = ay;
+                p.acc[3 * (size_t)o + 2] = az;
+                if (p.pot) p.pot[o] = T.pot[s].value();
+                if (p.oldacc_out) p.oldacc_out[li] = sqrt(ax * ax + ay * ay + az * az);
+            }
             if (p.ninter) p.ninter[o] = T.nint[s];
-            if (p.oldacc_out) p.oldacc_out[li] = sqrt(ax * ax + ay * ay + az * az);
             mycount += T.nint[s];
         }
 #pragma unroll
@@ -555,11 +573,11 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
     }
 }
 
-template <int TPL, int MINB, bool F64T>
+template <int TPL, int MINB, bool F64T, bool POT = false>
 static void launch_walk_t(const WalkParams &p, int blocks, int smem, cudaStream_t st)
 {
-    cudaFuncSetAttribute(k_walk<TPL, MINB, F64T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    k_walk<TPL, MINB, F64T><<<blocks, WALK_THREADS, smem, st>>>(p);
+    cudaFuncSetAttribute(k_walk<TPL, MINB, F64T, POT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k_walk<TPL, MINB, F64T, POT><<<blocks, WALK_THREADS, smem, st>>>(p);
 }
 
 // blocks_per_sm selects the register budget of the instantiation (1..3) and
@@ -569,7 +587,11 @@ void gg_launch_walk(const WalkParams &p, int tpl, int blocks_per_sm, cudaStream_
     int smem = gg_walk_smem_bytes(p.flush, tpl);
     int minb = blocks_per_sm < 1 ? 1 : (blocks_per_sm > 3 ? 3 : blocks_per_sm);
     int blocks = gg_num_sms() * blocks_per_sm;
-    if (p.group_size == 1) {
+    if (p.pot_only) {   // the potential-only walk: one register budget per mode
+        if (p.group_size == 1) launch_walk_t<1, 2, true, true>(p, blocks, smem, st);
+        else if (tpl == 2) launch_walk_t<2, 2, false, true>(p, blocks, smem, st);
+        else launch_walk_t<1, 2, false, true>(p, blocks, smem, st);
+    } else if (p.group_size == 1) {
         launch_walk_t<1, 2, true>(p, blocks, smem, st);   // exact mode: the reference's tests
     } else if (tpl == 2) {
         if (minb == 1) launch_walk_t<2, 1, false>(p, blocks, smem, st);

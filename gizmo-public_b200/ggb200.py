@@ -118,6 +118,9 @@ def load_library():
             "gg_load_velocities_device": (i32, [P, P]),
             "gg_drift": (i32, [P, dbl]),
             "gg_device_bytes": (i32, [P, ctypes.POINTER(i64)]),
+            "gg_evaluate_potential": (i32, [P, P, i64, P, dbl, dbl, P, ctypes.POINTER(Stats)]),
+            "gg_evaluate_potential_device": (i32, [P, P, i64, P, dbl, dbl, P]),
+            "gg_energy_device": (i32, [P, P, P, P]),
             "gg_reserve_device_pool": (i32, [i32, i64]),
             "gg_load_systems": (i32, [P, i32, P, P, P, P]),
             "gg_load_system_velocities": (i32, [P, P]),
@@ -324,6 +327,31 @@ class GravityTree:
         st = Stats()
         _check(self._lib.gg_fetch_results(self._h, _ptr(acc), _ptr(pot), ctypes.byref(st)), "gg_fetch_results")
         return acc, pot, st.as_dict()
+
+    def evaluate_potential(self, active=None, old_acc=None, err_tol_force_acc=0.0025, err_tol_theta=0.0):
+        """The potential-only walk (compute_potential), pre-G.  Returns (pot, stats)."""
+        act = None if active is None else np.ascontiguousarray(active, dtype=np.int32)
+        nt = self.n if act is None else act.shape[0]
+        pot = np.empty(nt)
+        oa = None if old_acc is None else np.ascontiguousarray(old_acc, dtype=np.float64)
+        st = Stats()
+        _check(self._lib.gg_evaluate_potential(self._h, None if act is None else act.ctypes.data, nt,
+                                               None if oa is None else oa.ctypes.data, err_tol_force_acc,
+                                               err_tol_theta, pot.ctypes.data, ctypes.byref(st)),
+               "gg_evaluate_potential")
+        return pot, st.as_dict()
+
+    def evaluate_potential_device(self, d_pot, d_active=None, n_active=0, d_old_acc=None, err_tol_force_acc=0.0025,
+                                  err_tol_theta=0.0):
+        _check(self._lib.gg_evaluate_potential_device(self._h, _ptr(d_active), n_active, _ptr(d_old_acc),
+                                                      err_tol_force_acc, err_tol_theta, _ptr(d_pot)),
+               "gg_evaluate_potential_device")
+
+    def energy_device(self, d_acc=None, d_pot=None):
+        """Per system [W = 1/2 sum m phi, sum m ax, sum m ay, sum m az] in FP64 (pre-G)."""
+        out = np.empty((len(self.counts), 4))
+        _check(self._lib.gg_energy_device(self._h, _ptr(d_acc), _ptr(d_pot), out.ctypes.data), "gg_energy_device")
+        return out
 
     def device_bytes(self):
         """Device memory the context holds now."""

@@ -147,6 +147,25 @@ gg_status gg_device_bytes(gg_ctx *ctx, int64_t *bytes);
  * (what was reserved until then stays reserved).  Synchronous. */
 gg_status gg_reserve_device_pool(int32_t device, int64_t bytes);
 
+/* ---- potential-only walk and energy checks -------------------------------
+ * compute_potential (gravity/potential.c:24-160) with its walk
+ * force_treeevaluate_potential (gravity/forcetree.c:3169-3474): the force
+ * walk's opening rules, the potential only, r = 0 pairs counted like any other
+ * pair, then each particle's self term m_i kernel(0) / h_i removed
+ * (potential.c:137-145).  Pre-G.  A given old_acc becomes the context's OldAcc
+ * as in gg_evaluate; the potential walk itself does not update OldAcc.
+ * gg_evaluate_potential blocks; the device form is asynchronous. */
+gg_status gg_evaluate_potential(gg_ctx *ctx, const int32_t *active, int64_t n_active, const double *old_acc,
+                                double err_tol_force_acc, double err_tol_theta, double *pot_out, gg_stats *stats);
+gg_status gg_evaluate_potential_device(gg_ctx *ctx, const int32_t *d_active, int64_t n_active,
+                                       const double *d_old_acc, double err_tol_force_acc, double err_tol_theta,
+                                       double *d_pot_out);
+/* FP64 checks per system over every particle, from load-order device arrays
+ * of all particles (either may be NULL): out[4 s] = W = 1/2 sum m phi (the
+ * potential energy of global.c:54, pre-G); out[4 s + 1..3] = sum m a, zero for
+ * exact forces of an isolated system.  Masses as stored (FP32).  Blocking. */
+gg_status gg_energy_device(gg_ctx *ctx, const double *d_acc, const double *d_pot, double *out);
+
 /* ---- drift of the resident tree ----------------------------------------
  * Re-evaluation between rebuilds, as GIZMO does when TreeReconstructFlag is
  * not set: particles move by Vel*dt (drift_particle, predict.c:97-137) and

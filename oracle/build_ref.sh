@@ -15,7 +15,7 @@ CC=/usr/bin/gcc
 # x86-64-v3 (AVX2/FMA): the binary runs on the GPU hosts as well as here
 CFLAGS="-O3 -march=x86-64-v3 -fopenmp -std=gnu99 -w"
 if [ ! -d "$REF" ]; then echo "reference tree not found: $REF" >&2; exit 1; fi
-if [ -x "$OUT/gizmo_ref" ] && [ -x "$OUT/gizmo_b200" ] && [ "$OUT/gizmo_b200" -nt "$HERE/ref_main.c" ] && [ "$OUT/gizmo_b200" -nt "$0" ] && [ "$OUT/gizmo_b200" -nt "$HERE/../gizmo-public_b200/host/gravtree_b200.c" ]; then
+if [ -x "$OUT/gizmo_ref" ] && [ -x "$OUT/gizmo_ref_pot" ] && [ -x "$OUT/gizmo_b200" ] && [ "$OUT/gizmo_b200" -nt "$HERE/ref_main.c" ] && [ "$OUT/gizmo_b200" -nt "$0" ] && [ "$OUT/gizmo_b200" -nt "$HERE/../gizmo-public_b200/host/gravtree_b200.c" ] && [ "$OUT/gizmo_ref_pot" -nt "$HERE/ref_main.c" ]; then
   echo "oracle/_ref/gizmo_ref is up to date"; exit 0
 fi
 MIRROR="$(mktemp -d /tmp/gg_ref_src.XXXXXX)"
@@ -57,6 +57,25 @@ $CC $CFLAGS -I"$HERE/shim" -c "$HERE/shim/mpi_single.c" -o "$OUT/obj/mpi_single.
 $CC $CFLAGS -I"$HERE/shim" -c "$HERE/shim/gsl_shim.c" -o "$OUT/obj/gsl_shim.o"
 $CC $CFLAGS -o "$OUT/gizmo_ref" $OBJS "$OUT/obj/ref_main.o" "$OUT/obj/mpi_single.o" "$OUT/obj/gsl_shim.o" -lm
 echo "built $OUT/gizmo_ref"
+# variant without EVALPOTENTIAL, with COMPUTE_POTENTIAL_ENERGY: it has the
+# separate potential-only walk (compute_potential) that the harness calls
+# after the start-up passes.  Output: oracle/_ref/gizmo_ref_pot.
+MIRROR_POT="$MIRROR/pot_tree"
+mkdir -p "$MIRROR_POT"
+cp -rs "$REF/." "$MIRROR_POT/"
+rm -f "$MIRROR_POT/GIZMO_config.h"
+cp "$HERE/shim/pot/GIZMO_config.h" "$MIRROR_POT/GIZMO_config.h"
+mkdir -p "$OUT/obj_pot"
+OBJS_POT=""
+for f in $FILES; do
+  o="$OUT/obj_pot/$(echo "$f" | tr / _ | sed 's/\.c$/.o/')"
+  OBJS_POT="$OBJS_POT $o"
+  echo "cd $MIRROR_POT && $CC $CFLAGS -I$HERE/shim -I$MIRROR_POT -c $f -o $o"
+done > "$MIRROR/cmds_pot.sh"
+xargs -P "$(nproc)" -I{} bash -c '{}' < "$MIRROR/cmds_pot.sh"
+$CC $CFLAGS -DGG_WITH_COMPUTE_POTENTIAL -I"$HERE/shim" -I"$MIRROR_POT" -c "$HERE/ref_main.c" -o "$OUT/obj_pot/ref_main.o"
+$CC $CFLAGS -o "$OUT/gizmo_ref_pot" $OBJS_POT "$OUT/obj_pot/ref_main.o" "$OUT/obj/mpi_single.o" "$OUT/obj/gsl_shim.o" -lm
+echo "built $OUT/gizmo_ref_pot"
 # GIZMO driving the B200 library through its C host code (needs the CUDA library)
 PKG="$(cd "$HERE/../gizmo-public_b200" && pwd)"
 if [ -f "$PKG/libgizmo_gravity_b200.so" ]; then

@@ -307,9 +307,13 @@ static void tree_moments(otree_t *t, int node)
     nd->multiple = count > 1;
 }
 
-/* one target's walk (forcetree.c:1823-2657); returns the interaction count */
+/* one target's walk (forcetree.c:1823-2657); returns the interaction count.
+ * pot_mode: the potential-only walk (force_treeevaluate_potential,
+ * forcetree.c:3169-3474), which has the same opening rules but no r2 > 0 or
+ * m > 0 condition on a pair: r = 0 pairs (the target itself, coincident
+ * particles) add m kernel(0) like any other. */
 static int64_t tree_walk(const otree_t *t, const double *pos, double soft, double aold, double theta, double *acc,
-                         double *pot_out)
+                         double *pot_out, int pot_mode)
 {
     int64_t n = t->n, nint = 0;
     double ax = 0, ay = 0, az = 0, pot = 0;
@@ -325,7 +329,7 @@ static int64_t tree_walk(const otree_t *t, const double *pos, double soft, doubl
             dz = t->pos[3 * no + 2] - pos[2];
             r2 = dx * dx + dy * dy + dz * dz;
             mass = t->mass[no];
-            if (r2 > 0 && mass > 0) h_p = t->h[no];
+            if ((r2 > 0 && mass > 0) || pot_mode) h_p = t->h[no];
         } else {
             const onode_t *nd = &t->nodes[no - n];
             int open = 0;
@@ -358,7 +362,7 @@ static int64_t tree_walk(const otree_t *t, const double *pos, double soft, doubl
             }
             h_p = nd->maxsoft;
         }
-        if (r2 > 0 && mass > 0) {
+        if ((r2 > 0 && mass > 0) || pot_mode) {
             pair_term(dx, dy, dz, r2, mass, h, h_p, &ax, &ay, &az, &pot);
             nint++;
         }
@@ -394,7 +398,7 @@ int64_t oracle_tree_gravity(int64_t n, const double *pos, const double *mass, co
     for (int64_t k = 0; k < n_targets; k++) {
         int64_t i = targets ? targets[k] : k;
         double aold = err_tol_force_acc * (old_acc ? old_acc[i] : 0.0);
-        int64_t c = tree_walk(&t, &pos[3 * i], h[i], aold, err_tol_theta, &acc[3 * k], &pot[k]);
+        int64_t c = tree_walk(&t, &pos[3 * i], h[i], aold, err_tol_theta, &acc[3 * k], &pot[k], 0);
         if (ninter) ninter[k] = c;
         total += c;
     }
@@ -439,7 +443,7 @@ int64_t oracle_tree_gravity_drift(int64_t n, const double *pos, const double *ve
     for (int64_t k = 0; k < n_targets; k++) {
         int64_t i = targets ? targets[k] : k;
         double aold = err_tol_force_acc * (old_acc ? old_acc[i] : 0.0);
-        int64_t c = tree_walk(&t, &moved[3 * i], h[i], aold, err_tol_theta, &acc[3 * k], &pot[k]);
+        int64_t c = tree_walk(&t, &moved[3 * i], h[i], aold, err_tol_theta, &acc[3 * k], &pot[k], 0);
         if (ninter) ninter[k] = c;
         total += c;
     }
@@ -447,6 +451,35 @@ int64_t oracle_tree_gravity_drift(int64_t n, const double *pos, const double *ve
     free(moved);
     free(t.nodes);
     return total;
+}
+
+/*
+ * compute_potential (gravity/potential.c:24-160) for an isolated tree-only
+ * run: the potential-only walk of every target, then its self term removed,
+ * m_i / h_i * kernel_gravity(0,1,1,-1) = -2.8 m_i / h_i (potential.c:137-145).
+ * Pre-G like P[].Potential before the multiplication by G.
+ */
+void oracle_potential(int64_t n, const double *pos, const double *mass, const double *h, const double *old_acc,
+                      double err_tol_force_acc, double err_tol_theta, int64_t n_targets, const int32_t *targets,
+                      double *pot, int nthreads)
+{
+    double center[3], corner[3], len;
+    oracle_find_extent(n, pos, center, corner, &len);
+    otree_t t = {n, pos, mass, h, NULL, NULL, 0, 0};
+    tree_build(&t, center, corner, len);
+    tree_moments(&t, 0);
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64)
+#endif
+    for (int64_t k = 0; k < n_targets; k++) {
+        int64_t i = targets ? targets[k] : k;
+        double aold = err_tol_force_acc * (old_acc ? old_acc[i] : 0.0);
+        double acc[3];
+        tree_walk(&t, &pos[3 * i], h[i], aold, err_tol_theta, acc, &pot[k], 1);
+        pot[k] -= mass[i] / h[i] * spline_gravity(0.0, 1.0, 1.0, -1);
+    }
+    free(t.nodes);
 }
 
 /* node count of the GIZMO octree (diagnostics) */

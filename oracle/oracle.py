@@ -40,6 +40,8 @@ def lib():
         L.oracle_tree_gravity.restype = i64
         L.oracle_tree_gravity_drift.argtypes = [i64, P, P, P, P, P, dbl, dbl, dbl, i64, P, P, P, P, P, ctypes.c_int]
         L.oracle_tree_gravity_drift.restype = i64
+        L.oracle_potential.argtypes = [i64, P, P, P, P, dbl, dbl, i64, P, P, ctypes.c_int]
+        L.oracle_potential.restype = None
         L.oracle_tree_nodes.argtypes = [i64, P, P, P]
         L.oracle_tree_nodes.restype = i64
         L.oracle_direct_sum.argtypes = [i64, P, P, P, i64, P, P, P, ctypes.c_int]
@@ -115,6 +117,20 @@ def tree_gravity_drift(pos, vel, mass, h, dt, old_acc=None, err_tol_force_acc=0.
                                             dt, nt, None if tg is None else tg.ctypes.data, acc.ctypes.data,
                                             pot.ctypes.data, nint.ctypes.data, moved.ctypes.data, nthreads)
     return acc, pot, nint, int(total), moved
+
+
+def potential(pos, mass, h, old_acc=None, err_tol_force_acc=0.0025, err_tol_theta=0.0, targets=None, nthreads=0):
+    """compute_potential: the potential-only walk with the self term removed (pre-G)."""
+    pos, mass, h = _c(pos, np.float64), _c(mass, np.float64), _c(h, np.float64)
+    n = pos.shape[0]
+    tg = None if targets is None else _c(targets, np.int32)
+    nt = n if tg is None else tg.shape[0]
+    oa = None if old_acc is None else _c(old_acc, np.float64)
+    pot = np.zeros(nt)
+    lib().oracle_potential(n, pos.ctypes.data, mass.ctypes.data, h.ctypes.data, None if oa is None else oa.ctypes.data,
+                           err_tol_force_acc, err_tol_theta, nt, None if tg is None else tg.ctypes.data, pot.ctypes.data,
+                           nthreads)
+    return pot
 
 
 def tree_nodes(pos, mass, h):

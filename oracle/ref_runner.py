@@ -22,6 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 BIN = os.path.join(HERE, "_ref", "gizmo_ref")
 # GIZMO driving the B200 library through gizmo-public_b200/host/gravtree_b200.c
 BIN_B200 = os.path.join(HERE, "_ref", "gizmo_b200")
+BIN_POT = os.path.join(HERE, "_ref", "gizmo_ref_pot")   # variant with compute_potential (no EVALPOTENTIAL)
 KERNEL_FAC = 2.8
 
 
@@ -197,6 +198,12 @@ def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeou
         kidx = order[kr["id"].astype(np.int64) - 1]
         keys_hi[kidx], keys_lo[kidx] = kr["hi"], kr["lo"]
         res_extra = {}
+        pot_path = os.path.join(d, "res.bin.pot")
+        if os.path.exists(pot_path):
+            pr = np.fromfile(pot_path, dtype=np.dtype([("id", "<u8"), ("v", "<f8")]))
+            pot_only = np.empty(n)
+            pot_only[order[pr["id"].astype(np.int64) - 1]] = pr["v"]
+            res_extra["pot_only"] = pot_only
         if drift_dt > 0:
             dr = np.fromfile(os.path.join(d, "res.bin.drift"), dtype=rec.dtype)
             out_dr = np.empty((n, 5))

@@ -8,7 +8,9 @@ outputs: root cube, 42-bit Peano-Hilbert keys (peano_hilbert_key), the
 Barnes-Hut pass and the relative pass (GravAccel, Potential; G = 1) and the
 interaction counts of both passes; then a re-evaluation after a drift of
 DRIFT_DT without a rebuild (drifted positions, forces, potentials and count),
-in which GIZMO's walk moves the tree nodes itself (force_drift_node).  Requires the reference source tree, so it
+in which GIZMO's walk moves the tree nodes itself (force_drift_node); and
+the potential-only walk (compute_potential) of the build variant without
+EVALPOTENTIAL, run on the same tree after the start-up passes.  Requires the reference source tree, so it
 runs only where that tree exists; the .npz files it writes are committed.
 """
 import os
@@ -37,6 +39,7 @@ def main():
     for name, (gen, tol) in CASES.items():
         ic = gen()
         r = ref_runner.run(ic, tol=tol, threads=1, drift_dt=DRIFT_DT)
+        rp = ref_runner.run(ic, tol=tol, threads=1, binary=ref_runner.BIN_POT)
         s = r["info"]["startup"]
         np.savez_compressed(
             os.path.join(HERE, name + ".npz"), pos=ic["pos"], mass=ic["mass"], h=ic["h"], tol=tol,
@@ -44,7 +47,8 @@ def main():
             key_hi=r["key_hi"], key_lo=r["key_lo"], acc_bh=r["acc_bh"], pot_bh=r["pot_bh"], acc=r["acc"],
             pot=r["pot"], oldacc=r["oldacc"], cost_bh=s["cost_bh"], cost_rel=s["cost_rel"], vel=ic["vel"],
             drift_dt=r["info"]["drift"]["dt"], pos_drift=r["pos_drift"], acc_drift=r["acc_drift"],
-            pot_drift=r["pot_drift"], cost_drift=r["info"]["drift"]["cost"])
+            pot_drift=r["pot_drift"], cost_drift=r["info"]["drift"]["cost"], pot_only=rp["pot_only"],
+            oldacc_pot=rp["oldacc"])
         print(name, "n=%d cost_bh=%d cost_rel=%d cost_drift=%d" % (ic["pos"].shape[0], s["cost_bh"], s["cost_rel"],
                                                                   r["info"]["drift"]["cost"]))
 

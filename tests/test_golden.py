@@ -137,3 +137,31 @@ def test_gpu_default_mode_after_drift_no_worse_than_reference(path):
     o50, o99, _ = ics.error_stats(a, acc_d)
     assert o50 <= 1.1 * r50 and o99 <= 1.1 * r99, (o50, o99, r50, r99)
     assert s["error_word"] == 0
+
+
+# ---- the potential-only walk (compute_potential, gravity/potential.c:24)
+@pytest.mark.parametrize("path", CASES, ids=IDS)
+def test_oracle_matches_reference_potential_walk(path):
+    g = load(path)
+    tol = float(g["tol"])
+    p = oracle.potential(g["pos"], g["mass"], g["h"], old_acc=g["oldacc_pot"], err_tol_force_acc=tol)
+    assert np.allclose(p, g["pot_only"], rtol=1e-12, atol=1e-14 * np.abs(g["pot_only"]).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", CASES, ids=IDS)
+def test_gpu_potential_walk_matches_reference(path):
+    g = load(path)
+    tol = float(g["tol"])
+    acc_d, pot_d = oracle.direct_sum(g["pos"], g["mass"], g["h"])
+    for leaf, group in ((1, 1), (8, 32)):
+        with ggb200.GravityTree(leaf_size=leaf, group_size=group) as t:
+            t.load(g["pos"], g["mass"], g["h"])
+            t.build()
+            p, st = t.evaluate_potential(old_acc=g["oldacc_pot"], err_tol_force_acc=tol)
+        assert st["error_word"] == 0
+        if group == 1:   # exact mode: the reference's walk in FP32 arithmetic
+            assert np.allclose(p, g["pot_only"], rtol=5e-5)
+        # W = 1/2 sum m phi no further from the direct sum than the reference's
+        W, Wd, Wr = (0.5 * np.sum(g["mass"] * q) for q in (p, pot_d, g["pot_only"]))
+        assert abs(W - Wd) <= max(1.1 * abs(Wr - Wd), 1e-5 * abs(Wd)), (leaf, W, Wd, Wr)
