@@ -1344,3 +1344,17 @@ extern "C" gg_status gg_energy_device(gg_ctx *c, const double *d_acc, const doub
     GG_CUDA_TRY(cudaStreamSynchronize(s));
     return GG_OK;
 }
+
+// ---------------------------------------------------------------- Peano-Hilbert order
+extern "C" gg_status gg_get_order(gg_ctx *c, int32_t *order_out)
+{
+    if (!c || !order_out) return GG_ERR_INVALID;
+    if (!c->built) return GG_ERR_NOT_BUILT;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    if (c->N == 0) return GG_OK;
+    // perm holds the load index of each sorted position (uint32 < 2^30)
+    GG_CUDA_TRY(cudaMemcpyAsync(order_out, c->perm.p, (size_t)c->N * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    GG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return GG_OK;
+}

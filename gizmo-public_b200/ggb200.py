@@ -118,6 +118,7 @@ def load_library():
             "gg_load_velocities_device": (i32, [P, P]),
             "gg_drift": (i32, [P, dbl]),
             "gg_device_bytes": (i32, [P, ctypes.POINTER(i64)]),
+            "gg_get_order": (i32, [P, P]),
             "gg_evaluate_potential": (i32, [P, P, i64, P, dbl, dbl, P, ctypes.POINTER(Stats)]),
             "gg_evaluate_potential_device": (i32, [P, P, i64, P, dbl, dbl, P]),
             "gg_energy_device": (i32, [P, P, P, P]),
@@ -351,6 +352,12 @@ class GravityTree:
         """Per system [W = 1/2 sum m phi, sum m ax, sum m ay, sum m az] in FP64 (pre-G)."""
         out = np.empty((len(self.counts), 4))
         _check(self._lib.gg_energy_device(self._h, _ptr(d_acc), _ptr(d_pot), out.ctypes.data), "gg_energy_device")
+        return out
+
+    def order(self):
+        """Load index of every sorted position of the last build (Peano-Hilbert order)."""
+        out = np.empty(self.n, dtype=np.int32)
+        _check(self._lib.gg_get_order(self._h, out.ctypes.data), "gg_get_order")
         return out
 
     def device_bytes(self):

@@ -97,6 +97,79 @@ static void gravtree_b200_drift(void)
     gg_tree_ti = All.Ti_Current;
 }
 
+/* Peano-Hilbert order of P[] on the GPU: replaces the sort of
+ * peano_hilbert_order (system/peano.c:28-92), called from
+ * domain_Decomposition (domain.c:275).  Gas cells [0, N_gas) and the other
+ * particles are ordered separately, as there, by their key in GIZMO's domain
+ * cube (DomainCorner, DomainLen); the library sorts the two blocks as two
+ * systems that share that cube.  The permutation is then applied in place by
+ * following its cycles, to P[] and, for gas, SphP[] (the reference's
+ * reorder_particles / reorder_gas do the same moves with their own index
+ * table).  Particles that share a 21-bit cell keep their relative order here
+ * (the reference orders them by finer key bits).  Invalidates the device tree:
+ * call it before the tree is built, as domain_Decomposition does. */
+static void gg_apply_order(const int32_t *order, long first, long n, int with_sph, int *dest)
+{
+    long k;
+    for (k = 0; k < n; k++) dest[order[first + k] - first] = (int)k;   /* new slot of each old slot */
+    for (k = 0; k < n; k++) {
+        while (dest[k] != k) {   /* send the record in slot k to its slot, take what was there */
+            int d = dest[k];
+            struct particle_data tp = P[first + d];
+            P[first + d] = P[first + k];
+            P[first + k] = tp;
+            if (with_sph) {
+                struct gas_cell_data ts = SphP[first + d];
+                SphP[first + d] = SphP[first + k];
+                SphP[first + k] = ts;
+            }
+            dest[k] = dest[d];
+            dest[d] = d;
+        }
+    }
+}
+
+void peano_hilbert_order_b200(void)
+{
+    gg_status st;
+    int i, k, S = 0;
+    if (!gg_tree_ctx) {
+        gg_config cfg;
+        gg_config_default(&cfg);
+        if ((st = gg_create(&cfg, &gg_tree_ctx))) gg_fail("gg_create", st);
+    }
+    gg_reserve(NumPart);
+    for (i = 0; i < NumPart; i++) gg_soft[i] = ForceSoftening_KernelRadius(i);
+    int64_t counts[2];
+    long first[2];
+    if (N_gas > 0) { counts[S] = N_gas; first[S] = 0; S++; }
+    if (NumPart - N_gas > 0) { counts[S] = NumPart - N_gas; first[S] = N_gas; S++; }
+    if (S == 0) return;
+    st = gg_load_particles(gg_tree_ctx, S, counts, &P[0].Pos[0], (int64_t)sizeof(struct particle_data), &P[0].Mass,
+                           (int64_t)sizeof(struct particle_data), gg_soft, (int64_t)sizeof(double));
+    if (st) gg_fail("gg_load_particles", st);
+    gg_domain dom[2];
+    for (k = 0; k < S; k++) {
+        int j;
+        for (j = 0; j < 3; j++) {
+            dom[k].center[j] = DomainCenter[j];
+            dom[k].corner[j] = DomainCorner[j];
+        }
+        dom[k].len = DomainLen;
+    }
+    if ((st = gg_build(gg_tree_ctx, dom))) gg_fail("gg_build", st);
+    int32_t *order = (int32_t *)malloc(sizeof(int32_t) * (NumPart ? NumPart : 1));
+    int *dest = (int *)malloc(sizeof(int) * (NumPart ? NumPart : 1));
+    if (!order || !dest) {
+        printf("B200 gravity: host allocation for the Peano-Hilbert order failed\n");
+        endrun(3134);
+    }
+    if ((st = gg_get_order(gg_tree_ctx, order))) gg_fail("gg_get_order", st);
+    for (k = 0; k < S; k++) gg_apply_order(order, first[k], (long)counts[k], first[k] == 0 && N_gas > 0, dest);
+    free(dest);
+    free(order);
+}
+
 /* Local walk: replaces the force_treeevaluate loop over the active particles
  * (gravtree.c:138-457).  Leaves the pre-G force and potential in P[] like the
  * reference's walk does (forcetree.c:2661-2701) and returns the interaction

@@ -117,6 +117,13 @@ gg_status gg_load_particles_device(gg_ctx *ctx, int32_t n_systems, const int64_t
  * root cube of each system is found on the device like domain_findExtent. */
 gg_status gg_build(gg_ctx *ctx, const gg_domain *domains);
 gg_status gg_get_domains(gg_ctx *ctx, gg_domain *out);
+/* The Peano-Hilbert order of the last build: order_out[i] = load index of
+ * the particle at sorted position i (N entries; systems in load order, each
+ * sorted by key, ties by load index).  With GIZMO's domain cube passed to
+ * gg_build this is peano_hilbert_order's sort (system/peano.c:28-92) down to
+ * 21 bits per dimension; the reference orders particles that share a 21-bit
+ * cell by its finer key bits.  Blocking. */
+gg_status gg_get_order(gg_ctx *ctx, int32_t *order_out);
 
 /* ---- walk --------------------------------------------------------------
  * The force_treeevaluate loop of gravity_tree (gravtree.c:138-457).

@@ -214,6 +214,8 @@ def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeou
             res_extra = {"acc_drift": out_dr[:, :3], "pot_drift": out_dr[:, 3], "oldacc_drift": out_dr[:, 4],
                          "pos_drift": pos_dr}
         for line in r.stdout.decode().splitlines():
+            if line.startswith("phorder"):
+                info["phorder"] = {k: int(v) for k, v in (p.split("=", 1) for p in line.split()[1:])}
             if line.startswith("drift"):
                 kv = dict(p.split("=", 1) for p in line.split()[1:])
                 info["drift"] = {k: float(v) for k, v in kv.items()}

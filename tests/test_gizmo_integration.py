@@ -46,3 +46,18 @@ def test_gizmo_with_b200_gravity_matches_reference(model):
     r50, r99, _ = ics.error_stats(ref["acc_drift"], acc_dd)
     g50, g99, _ = ics.error_stats(gpu["acc_drift"], acc_dd)
     assert g50 <= 1.1 * r50 and g99 <= 1.1 * r99, (g50, g99, r50, r99)
+
+
+@pytest.mark.skipif(not ref_runner.available(ref_runner.BIN_B200),
+                    reason="reference binaries not built (oracle/build_ref.sh needs the reference tree)")
+@pytest.mark.parametrize("model", ["plummer", "galaxy"])
+def test_gizmo_peano_hilbert_order_on_the_gpu(model, monkeypatch):
+    """peano_hilbert_order_b200() inside GIZMO: after a shuffle of P[] it
+    restores GIZMO's own order down to 21-bit cells (the harness compares the
+    key prefixes along both orders with GIZMO's own key function)."""
+    ic = ics.plummer(20000, seed=211) if model == "plummer" else ics.galaxy(n_halo=12000, n_disk=8000, seed=212)
+    monkeypatch.setenv("GG_CHECK_PH_ORDER", "1")
+    r = ref_runner.run(ic, threads=4, binary=ref_runner.BIN_B200)
+    ph = r["info"]["phorder"]
+    assert ph["n"] == ic["pos"].shape[0] and ph["moved"] > ph["n"] // 2
+    assert ph["key21_sorted"] == 1 and ph["same_as_reference"] == 1

@@ -165,3 +165,20 @@ def test_gpu_potential_walk_matches_reference(path):
         # W = 1/2 sum m phi no further from the direct sum than the reference's
         W, Wd, Wr = (0.5 * np.sum(g["mass"] * q) for q in (p, pot_d, g["pot_only"]))
         assert abs(W - Wd) <= max(1.1 * abs(Wr - Wd), 1e-5 * abs(Wd)), (leaf, W, Wd, Wr)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", CASES, ids=IDS)
+def test_gpu_order_is_the_reference_key_order(path):
+    """gg_get_order: the sorted positions follow the reference's 42-bit keys
+    down to 21 bits per dimension, ties in load order."""
+    g = load(path)
+    with ggb200.GravityTree() as t:
+        t.load(g["pos"], g["mass"], g["h"])
+        t.build()
+        order = t.order()
+    assert np.array_equal(np.sort(order), np.arange(order.size))
+    k21 = (g["key_hi"][order] << np.uint64(1)) | (g["key_lo"][order] >> np.uint64(63))
+    assert np.all(k21[1:] >= k21[:-1])
+    same = k21[1:] == k21[:-1]
+    assert np.all(order[1:][same] > order[:-1][same])
