@@ -532,6 +532,70 @@ def run_serve(args, torch, ggb200, dist, world, rank, local):
     return 0
 
 
+# ---------------------------------------------------------------- one system over the ranks
+def run_split(args, torch, ggb200, dist, world, rank, local):
+    """Strong scaling: one system of the workload, an equal share per rank;
+    a step all-gathers the 32-byte records (NCCL), builds the whole tree on
+    every rank and walks the rank's own particles (multi.SplitSystem)."""
+    name, gen = WORKLOADS[args.workload]
+    ic = gen(SEEDS[args.workload])             # the same system on every rank
+    n = ic["pos"].shape[0]
+    share = [n // world + (1 if r < n % world else 0) for r in range(world)]
+    off = sum(share[:rank])
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    rec = ggb200.make_records(ic["pos"][off:off + share[rank]], ic["mass"][off:off + share[rank]],
+                              ic["h"][off:off + share[rank]])
+    d_rec = torch.from_numpy(rec.view(np.uint8)).to(dev)
+    d_acc = torch.empty((share[rank], 3), dtype=torch.float64, device=dev)
+    d_pot = torch.empty(share[rank], dtype=torch.float64, device=dev)
+    tree = ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush, device=local,
+                              blocks_per_sm=args.blocks_per_sm, target_order=args.target_order)
+    tree.set_stream(stream.cuda_stream)
+    split = multi.SplitSystem(dist, tree, torch, dev)
+    split.step(d_rec, d_acc, d_pot, err_tol_theta=0.7)
+    for _ in range(args.warmup):
+        split.step(d_rec, d_acc, d_pot, err_tol_force_acc=args.tol)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = ggb200.kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        split.step(d_rec, d_acc, d_pot, err_tol_force_acc=args.tol)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = ggb200.kernel_launches() - launches0
+    clk = clocks.stop()
+    ms_step = multi.max_over_ranks(dist, e0.elapsed_time(e1), device=dev) / args.steps
+    st = tree.last_stats()
+    out = {
+        "metric": METRIC, "value": n / (ms_step * 1e-3), "unit": "particles/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": name, "n": n, "share": share, "err_tol_force_acc": args.tol,
+                   "step": "all-gather of 32-byte records + extent+keys+sort+permute+tree+moments on every rank + "
+                           "relative walk of the rank's own particles",
+                   "parallelism": "one system over %d GPUs" % world},
+        "interactions_per_particle_rank0": st["interactions"] / max(share[rank], 1),
+        "clocks": clk, "gpu_launches": int(launches), "e2e": None, "cpu_baseline": None,
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    tree.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
 # ---------------------------------------------------------------- GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -558,6 +622,9 @@ def main():
     # individual timesteps: the timed walk evaluates a seeded random fraction of
     # the particles (the tree is still built over all of them)
     ap.add_argument("--active-frac", type=float, default=1.0)
+    # one system shared by the ranks (strong scaling): each rank holds an equal
+    # share, all-gathers the records each step and walks its own particles
+    ap.add_argument("--split", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -574,6 +641,8 @@ def main():
         return run_ensemble(args, torch, ggb200, dist, world, rank, local)
     if args.workload == "serve":
         return run_serve(args, torch, ggb200, dist, world, rank, local)
+    if args.split:
+        return run_split(args, torch, ggb200, dist, world, rank, local)
 
     name, gen = WORKLOADS[args.workload]
     ic = gen(multi.rank_seed(SEEDS[args.workload], rank))   # independent system per rank

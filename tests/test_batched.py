@@ -112,3 +112,35 @@ def test_autotune_keeps_the_force_error_and_returns_a_valid_config():
         tuned = _per_system_p99(ic, acc.cpu().numpy())
         assert tuned < 2e-3 and tuned <= 1.5 * base + 1e-4
         t.close()
+
+
+def test_split_system_step_on_one_gpu_equals_plain_evaluation():
+    """multi.SplitSystem at world size 1 (the gather is the identity): the
+    own-range walk through an active list equals the plain walk."""
+    import torch
+    import multi
+    ic = ics.galaxy(n_halo=14000, n_disk=6000, seed=13)
+    n = ic["pos"].shape[0]
+    rec = torch.from_numpy(ggb200.make_records(ic["pos"], ic["mass"], ic["h"]).view(np.uint8)).cuda()
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        ta = ggb200.GravityTree()
+        ta.set_stream(stream.cuda_stream)
+        split = multi.SplitSystem(None, ta, torch, "cuda")
+        acc_a = torch.empty((n, 3), dtype=torch.float64, device="cuda")
+        pot_a = torch.empty(n, dtype=torch.float64, device="cuda")
+        split.step(rec, acc_a, pot_a, err_tol_theta=0.7)
+        split.step(rec, acc_a, pot_a, err_tol_force_acc=0.001)
+        tb = ggb200.GravityTree()
+        tb.set_stream(stream.cuda_stream)
+        acc_b = torch.empty((n, 3), dtype=torch.float64, device="cuda")
+        pot_b = torch.empty(n, dtype=torch.float64, device="cuda")
+        tb.load_device(rec, [n])
+        tb.build()
+        tb.evaluate_device(acc_b, pot_b, err_tol_theta=0.7)
+        tb.build()
+        tb.evaluate_device(acc_b, pot_b, err_tol_force_acc=0.001)
+        torch.cuda.synchronize()
+        assert torch.equal(acc_a, acc_b) and torch.equal(pot_a, pot_b)
+        ta.close()
+        tb.close()
