@@ -33,6 +33,11 @@ import ics  # noqa: E402
 import multi  # noqa: E402
 
 FLOPS_PER_INTERACTION = 20   # monopole force convention (3 sub, r^2, rsqrt, m/r^3, 3 fma)
+# DRAM bytes (read + write) per particle of one k_walk launch on the galaxy,
+# from the ncu capture of the 1,000,000-particle galaxy (79.6 MB read + 23.0 MB
+# written); the walk's traffic grows with the particle count, so a launch of
+# the 4.2M galaxy is scaled from it
+WALK_DRAM_BYTES_PER_PARTICLE = {"galaxy": 102.6, "galaxy1m": 102.6}
 METRIC = "tree-gravity particles/s at p99 force err<=2e-3 vs FP64 direct; serve p50/p99 ms"
 
 WORKLOADS = {
@@ -819,7 +824,10 @@ def main():
                      "walk": stages["ms_walk"], "timed_build_phase": build_ms, "timed_walk_phase": walk_ms},
         "roofline": {"bound": "fp32", "kernel": "k_walk", "achieved": walk_tflops, "peak": peak32,
                      "unit": "TFLOP/s", "frac": (walk_tflops / peak32) if walk_tflops else None,
-                     "traffic": None, "flops_per_interaction": FLOPS_PER_INTERACTION,
+                     "traffic": (WALK_DRAM_BYTES_PER_PARTICLE[args.workload] * n
+                                 if args.workload in WALK_DRAM_BYTES_PER_PARTICLE else None),
+                     "traffic_source": "ncu dram bytes of one k_walk launch on the 1M galaxy, scaled by N",
+                     "flops_per_interaction": FLOPS_PER_INTERACTION,
                      "peak_source": "measured FP32 FMA probe (gg_fp32_peak_probe) on this GPU",
                      "timed_phase_achieved": walk_phase_tflops},
         "roofline_sort": {"bound": "hbm", "achieved": sort_gbs, "peak": hbm_peak, "unit": "GB/s",

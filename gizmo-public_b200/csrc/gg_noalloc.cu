@@ -10,7 +10,7 @@
 // variant takes its scratch from one file-scope __device__ array instead.
 //
 // The array holds at most GG_NOALLOC_SORT_MAX_N pairs' scratch; every GPU that
-// loads this library keeps it (about 16 MB) until the process exits.  All
+// loads this library keeps it (about 20 MB) until the process exits.  All
 // calls share it and it keeps the previous call's contents: the call clears
 // what must start at zero (histograms, tile counters, status words, error
 // word).  Two calls whose work overlaps on the GPU (on different streams, or
@@ -21,8 +21,8 @@
 #include "gg_kernels.cuh"
 
 // scratch of gg_sort_pairs_run for GG_NOALLOC_SORT_MAX_N pairs and 8 passes
-// (≈14.1 MB), plus the error word in the last 256 bytes
-#define GG_NOALLOC_SCRATCH_BYTES (16u << 20)
+// (≈16.0 MB with 2048-key tiles), plus the error word in the last 256 bytes
+#define GG_NOALLOC_SCRATCH_BYTES (20u << 20)
 
 static __device__ __align__(256) unsigned char gg_noalloc_scratch[GG_NOALLOC_SCRATCH_BYTES];
 

@@ -3,7 +3,7 @@
 // Replaces the reference's stable mergesort of {peanokey, index} records
 // (mysort_peano, system/peano.c:414-462; mysort_domain, domain.c:2674-2723).
 // Design (one-sweep): one up-front pass builds the digit histograms of every
-// pass; each pass is then a single kernel in which a CTA ranks a 4096-key tile
+// pass; each pass is then a single kernel in which a CTA ranks a 2048-key tile
 // in shared memory, publishes its per-digit counts, sums its predecessors'
 // counts with a decoupled look-back, and writes the tile out digit-sorted so
 // that global stores are contiguous runs.  8-bit digits.  For several systems
@@ -18,7 +18,7 @@
 #include "gg_kernels.cuh"
 
 #define SORT_THREADS 256
-#define SORT_ITEMS 16
+#define SORT_ITEMS 8      // 2048-key tiles: 4 blocks of 8 warps fit an SM (registers and shared memory)
 #define SORT_TILE (SORT_THREADS * SORT_ITEMS)
 #define SORT_WARPS (SORT_THREADS / 32)
 #define RADIX 256
@@ -96,7 +96,7 @@ __device__ __forceinline__ void st_status(unsigned *p, unsigned v)
 }
 
 // one pass: digit = (key >> shift) & 255, or (system id >> shift) & 255 when sys_mode
-__global__ void __launch_bounds__(SORT_THREADS) k_sort_pass(
+__global__ void __launch_bounds__(SORT_THREADS, 4) k_sort_pass(
     const unsigned long long *__restrict__ kin, const unsigned *__restrict__ vin, unsigned long long *__restrict__ kout,
     unsigned *__restrict__ vout, int n, int shift, int sys_mode, const int *__restrict__ poff, int S,
     const unsigned *__restrict__ g_off, unsigned *status, unsigned *tile_counter, int *err)
@@ -144,10 +144,7 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_pass(
         unsigned peers = __match_any_sync(0xffffffffu, d);
         int leader = __ffs(peers) - 1;
         unsigned base = 0;
-        if (lane == leader) {
-            base = s_whist[w][d];
-            s_whist[w][d] = base + __popc(peers);
-        }
+        if (lane == leader) base = atomicAdd(&s_whist[w][d], (unsigned)__popc(peers));
         base = __shfl_sync(peers, base, leader);
         rank[j] = base + __popc(peers & lt_mask);
         __syncwarp();

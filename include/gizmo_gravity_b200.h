@@ -251,7 +251,7 @@ gg_status gg_radix_sort_pairs(int64_t n, uint64_t *d_keys, uint32_t *d_vals, int
  * allocator, a serving loop admitting work against a fixed memory budget)
  * would see cudaMalloc fail or bypass its accounting, and a latency-critical
  * loop cannot take cudaFree's implicit device synchronisation.  The scratch is
- * one static device array of the library (about 16 MB, held by every GPU that
+ * one static device array of the library (about 20 MB, held by every GPU that
  * loads the library until the process exits), so n is limited to
  * GG_NOALLOC_SORT_MAX_N; larger n returns GG_ERR_TOO_LARGE.  The first call on
  * a device looks up the array's device address; make that first call before
