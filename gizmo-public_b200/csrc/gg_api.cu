@@ -172,6 +172,11 @@ static void parallel_copy(void *dst, const void *src, size_t bytes)
     }
 }
 
+// Host transfers of large arrays are cut into chunks of this many particles:
+// the host gathers or copies one chunk while the previous one crosses the link.
+static const long long kPipeChunk = 1ll << 20;
+static const int kPipeEvents = 64;
+
 struct gg_ctx {
     gg_config cfg;
     int device = 0;
@@ -245,6 +250,7 @@ struct gg_ctx {
     long long async_n = 0;
     int async_flags = 0;
     cudaEvent_t act_ev = nullptr, done_ev = nullptr;
+    cudaEvent_t pipe_ev[kPipeEvents] = {};   // completion of each chunk of a pipelined copy to the host
     gg_stats last;
 
     // every device buffer of the context, for release and accounting
@@ -355,6 +361,12 @@ extern "C" gg_status gg_create(const gg_config *cfg, gg_ctx **out)
         gg_destroy(ctx);
         return gg_cuda_fail(e);
     }
+    for (int i = 0; i < kPipeEvents; i++) {
+        if ((e = cudaEventCreateWithFlags(&ctx->pipe_ev[i], cudaEventDisableTiming)) != cudaSuccess) {
+            gg_destroy(ctx);
+            return gg_cuda_fail(e);
+        }
+    }
     for (int i = 0; i < 8; i++) cudaEventCreate(&ctx->ev[i]);
     ctx->have_events = true;
     memset(&ctx->last, 0, sizeof ctx->last);
@@ -381,6 +393,8 @@ extern "C" gg_status gg_destroy(gg_ctx *c)
     c->h_vstage.give_back(c->vstage_ev);
     c->h_stage.give_back(c->stage_ev);
     if (c->act_ev) cudaEventDestroy(c->act_ev);
+    for (int i = 0; i < kPipeEvents; i++)
+        if (c->pipe_ev[i]) cudaEventDestroy(c->pipe_ev[i]);
     if (c->done_ev) cudaEventDestroy(c->done_ev);
     if (c->stage_ev) cudaEventDestroy(c->stage_ev);
     if (c->vstage_ev) cudaEventDestroy(c->vstage_ev);
@@ -458,20 +472,24 @@ extern "C" gg_status gg_load_particles(gg_ctx *c, int32_t S, const int64_t *coun
     const char *pb = (const char *)pos, *mb = (const char *)mass, *hb = (const char *)soft_h;
     GGPart *dst = c->h_stage.p;
     int mixed = 0;
+    for (long long b = 0; b < N; b += kPipeChunk) {   // gather one chunk while the previous one is copied
+        const long long e = std::min(N, b + kPipeChunk);
 #pragma omp parallel for schedule(static) reduction(| : mixed)
-    for (long long i = 0; i < N; i++) {
-        const double *x = (const double *)(pb + i * pos_stride);
-        GGPart r;
-        r.x = x[0]; r.y = x[1]; r.z = x[2];
-        r.m = (float)*(const double *)(mb + i * mass_stride);
-        r.h = (float)*(const double *)(hb + i * soft_stride);
-        dst[i] = r;
-        if (i > 0 && r.h != (float)*(const double *)(hb + (i - 1) * soft_stride)) mixed = 1;
+        for (long long i = b; i < e; i++) {
+            const double *x = (const double *)(pb + i * pos_stride);
+            GGPart r;
+            r.x = x[0]; r.y = x[1]; r.z = x[2];
+            r.m = (float)*(const double *)(mb + i * mass_stride);
+            r.h = (float)*(const double *)(hb + i * soft_stride);
+            dst[i] = r;
+            if (i > 0 && r.h != (float)*(const double *)(hb + (i - 1) * soft_stride)) mixed = 1;
+        }
+        GG_CUDA_TRY(cudaMemcpyAsync(c->in_rec.p + b, dst + b, (e - b) * sizeof(GGPart), cudaMemcpyHostToDevice,
+                                    c->stream));
     }
     // a change of kernel radius between neighbouring particles of different
     // systems also counts: harmless (ordering then just keeps each system's order)
     c->h_mixed = mixed != 0;
-    if (N) GG_CUDA_TRY(cudaMemcpyAsync(c->in_rec.p, c->h_stage.p, N * sizeof(GGPart), cudaMemcpyHostToDevice, c->stream));
     GG_CUDA_TRY(cudaEventRecord(c->stage_ev, c->stream));
     return GG_OK;
 }
@@ -761,29 +779,49 @@ extern "C" gg_status gg_evaluate(gg_ctx *c, const int32_t *active, int64_t n_act
     }
     if (old_acc) {
         if ((st = c->h_old.ensure((size_t)c->N, c->done_ev))) return st;
-        parallel_copy(c->h_old.p, old_acc, (size_t)c->N * sizeof(double));
-        GG_CUDA_TRY(cudaMemcpyAsync(c->oldacc.p, c->h_old.p, c->N * sizeof(double), cudaMemcpyHostToDevice, s));
+        for (long long b = 0; b < c->N; b += kPipeChunk) {
+            const long long e = std::min((long long)c->N, b + kPipeChunk);
+            parallel_copy(c->h_old.p + b, old_acc + b, (size_t)(e - b) * sizeof(double));
+            GG_CUDA_TRY(cudaMemcpyAsync(c->oldacc.p + b, c->h_old.p + b, (e - b) * sizeof(double),
+                                        cudaMemcpyHostToDevice, s));
+        }
         c->oldacc_valid = true;
     }
     if ((st = run_walk(c, d_active, (int)n_active, nullptr, tol, theta, c->acc_d.p, c->pot_d.p, c->nint_d.p)))
         return st;
+    // results come back in chunks; each chunk is copied out while the next crosses the link
+    long long chunk = kPipeChunk, nchunks = 0;
     if (nt) {
         if ((st = c->h_acc.ensure((size_t)nt * 3, c->done_ev))) return st;
-        GG_CUDA_TRY(cudaMemcpyAsync(c->h_acc.p, c->acc_d.p, nt * 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
-        if (pot_out) {
-            if ((st = c->h_pot.ensure((size_t)nt, c->done_ev))) return st;
-            GG_CUDA_TRY(cudaMemcpyAsync(c->h_pot.p, c->pot_d.p, nt * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (pot_out && (st = c->h_pot.ensure((size_t)nt, c->done_ev))) return st;
+        if (ninter_out && (st = c->h_nint.ensure((size_t)nt, c->done_ev))) return st;
+        nchunks = (nt + chunk - 1) / chunk;
+        if (nchunks > kPipeEvents) {
+            chunk = (nt + kPipeEvents - 1) / kPipeEvents;
+            nchunks = (nt + chunk - 1) / chunk;
         }
-        if (ninter_out) {
-            if ((st = c->h_nint.ensure((size_t)nt, c->done_ev))) return st;
-            GG_CUDA_TRY(cudaMemcpyAsync(c->h_nint.p, c->nint_d.p, nt * sizeof(int), cudaMemcpyDeviceToHost, s));
+        for (long long k = 0; k < nchunks; k++) {
+            const long long b = k * chunk, e = std::min(nt, b + chunk);
+            GG_CUDA_TRY(cudaMemcpyAsync(c->h_acc.p + 3 * b, c->acc_d.p + 3 * b, (e - b) * 3 * sizeof(double),
+                                        cudaMemcpyDeviceToHost, s));
+            if (pot_out)
+                GG_CUDA_TRY(cudaMemcpyAsync(c->h_pot.p + b, c->pot_d.p + b, (e - b) * sizeof(double),
+                                            cudaMemcpyDeviceToHost, s));
+            if (ninter_out)
+                GG_CUDA_TRY(cudaMemcpyAsync(c->h_nint.p + b, c->nint_d.p + b, (e - b) * sizeof(int),
+                                            cudaMemcpyDeviceToHost, s));
+            GG_CUDA_TRY(cudaEventRecord(c->pipe_ev[k], s));
         }
     }
     GG_CUDA_TRY(cudaEventRecord(c->done_ev, s));
+    for (long long k = 0; k < nchunks; k++) {
+        const long long b = k * chunk, e = std::min(nt, b + chunk);
+        GG_CUDA_TRY(cudaEventSynchronize(c->pipe_ev[k]));
+        parallel_copy(acc_out + 3 * b, c->h_acc.p + 3 * b, (size_t)(e - b) * 3 * sizeof(double));
+        if (pot_out) parallel_copy(pot_out + b, c->h_pot.p + b, (size_t)(e - b) * sizeof(double));
+    }
     st = collect_stats(c, stats);   // synchronises the stream
     if (nt) {
-        parallel_copy(acc_out, c->h_acc.p, (size_t)nt * 3 * sizeof(double));
-        if (pot_out) parallel_copy(pot_out, c->h_pot.p, (size_t)nt * sizeof(double));
         if (ninter_out) {
             const int *ni = c->h_nint.p;
 #pragma omp parallel for schedule(static)
@@ -991,12 +1029,16 @@ extern "C" gg_status gg_load_velocities(gg_ctx *c, const double *vel, int64_t ve
     if ((st = c->h_vstage.ensure((size_t)N * 3, c->vstage_ev))) return st;
     const char *vb = (const char *)vel;
     double *dst = c->h_vstage.p;
+    for (long long b = 0; b < N; b += kPipeChunk) {
+        const long long e = std::min(N, b + kPipeChunk);
 #pragma omp parallel for schedule(static)
-    for (long long i = 0; i < N; i++) {
-        const double *v = (const double *)(vb + i * vel_stride);
-        dst[3 * i] = v[0]; dst[3 * i + 1] = v[1]; dst[3 * i + 2] = v[2];
+        for (long long i = b; i < e; i++) {
+            const double *v = (const double *)(vb + i * vel_stride);
+            dst[3 * i] = v[0]; dst[3 * i + 1] = v[1]; dst[3 * i + 2] = v[2];
+        }
+        GG_CUDA_TRY(cudaMemcpyAsync(c->vel.p + 3 * b, dst + 3 * b, (size_t)(e - b) * 3 * sizeof(double),
+                                    cudaMemcpyHostToDevice, c->stream));
     }
-    if (N) GG_CUDA_TRY(cudaMemcpyAsync(c->vel.p, dst, (size_t)N * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     GG_CUDA_TRY(cudaEventRecord(c->vstage_ev, c->stream));
     c->have_vel = true;
     c->kin_valid = false;
