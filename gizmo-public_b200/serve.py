@@ -85,8 +85,14 @@ class Server:
         self.cfg = dict(leaf_size=leaf, group_size=group, flush=flush, device=device)
         self.tree_factory = tree_factory or ggb200.GravityTree
         if reserve:
-            # map the whole budget once, before the first request
-            ggb200.reserve_device_pool(self.budget, device)
+            # map the whole budget once, before the first request; a device
+            # smaller than the budget keeps what it could map, and admission
+            # against the budget still holds
+            try:
+                ggb200.reserve_device_pool(self.budget, device)
+            except ggb200.GravityError as e:
+                if e.status != -3:   # GG_ERR_NOMEM
+                    raise
         self.pending_new = collections.deque()
         self.pending_re = collections.deque()
         self.resident = {}           # system id -> (_Context, index in context)
