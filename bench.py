@@ -609,8 +609,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="galaxy", choices=sorted(WORKLOADS) + ["ensemble", "serve"])
-    # 0.001 keeps the galaxy's p99 force error below 2e-3 (the metric's bound)
-    ap.add_argument("--tol", type=float, default=0.001)
+    # ErrTolForceAcc; by default per workload, the largest of 0.001 and 0.0008
+    # that keeps the p99 force error below 2e-3 (the metric's bound) with a margin:
+    # at 0.001 the galaxy's p99 is 1.77e-3 but the clustered system's 2.0e-3
+    ap.add_argument("--tol", type=float, default=None)
     ap.add_argument("--err-targets", type=int, default=65536)
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     ap.add_argument("--ref-sample", type=int, default=16384)
@@ -632,6 +634,8 @@ def main():
     ap.add_argument("--split", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.tol is None:
+        args.tol = 0.0008 if args.workload.startswith("clustered") else 0.001
 
     if args.impl == "reference":
         return run_reference_arm(args)
