@@ -156,6 +156,8 @@ def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if args.workload in ("ensemble", "serve"):
+        return run_reference_arm_systems(args)
     name, gen = WORKLOADS[args.workload]
     ic = gen(SEEDS[args.workload])
     n = ic["pos"].shape[0]
@@ -598,6 +600,40 @@ def run_split(args, torch, ggb200, dist, world, rank, local):
     tree.close()
     if dist:
         dist.destroy_process_group()
+    return 0
+
+
+def run_reference_arm_systems(args):
+    """Reference arm of the many-system workloads: the compiled reference run on
+    whole systems of the workload, one process per system, W+K samples of
+    systems; particles/s = sum of N / sum of step times."""
+    if args.workload == "ensemble":
+        ic = ics.ensemble(seed=ics.SEED_ENSEMBLE)
+        counts = ic["counts"]
+        off = np.concatenate([[0], np.cumsum(counts)])
+        rng = np.random.default_rng(77)
+        systems = []
+        for _ in range(args.warmup + args.steps):
+            s = int(rng.integers(0, counts.size))
+            systems.append({k: ic[k][int(off[s]):int(off[s + 1])] for k in ("pos", "vel", "mass", "h")})
+        name, what = ENSEMBLE_NAME, "ensemble"
+    else:
+        pool = sorted(ics.serving_pool(n_systems=128, seed=ics.SEED_SERVING), key=lambda x: x["pos"].shape[0])
+        systems = [pool[k] for k in range(0, 64, max(1, 64 // (args.warmup + args.steps)))][:args.warmup + args.steps]
+        name, what = SERVE_NAME, "serving pool"
+    info = systems_reference_rate(systems[args.warmup:], args.tol, what)
+    if info is None:
+        print(json.dumps({"impl": "reference", "unavailable": "compiled reference (oracle/_ref) not built"}))
+        return 0
+    v = info["value"]
+    out = {"metric": METRIC, "value": v, "unit": "particles/s", "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": name, "err_tol_force_acc": args.tol}, "impl": "reference",
+           "cpu_baseline": {"value": v, "unit": "particles/s", "cores": info["cores"], "kind": info["kind"],
+                            "sample": info["sample"]},
+           "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
     return 0
 
 
