@@ -39,7 +39,7 @@
 int gg_walk_threads() { return WALK_THREADS; }
 
 // Per-warp shared memory, in float4 units:
-//   far list float4[cap] | near list float4[cap] | near (h, 1/h) float2[cap] |
+//   far list float4[cap] | near list float4[cap] | near softening float4[cap] |
 //   node stack int[WALK_SSTACK]
 // with cap = flush + 32.  The stack spills to the warp's global stack area
 // when it overflows (deep or wide traversals only).
@@ -47,7 +47,7 @@ int gg_walk_threads() { return WALK_THREADS; }
 __host__ __device__ __forceinline__ int walk_warp_float4s(int flush)
 {
     const int cap = flush + 32;
-    return 2 * cap + (cap + 1) / 2 + WALK_SSTACK / 4;
+    return 3 * cap + WALK_SSTACK / 4;
 }
 
 int gg_walk_smem_bytes(int flush, int tpl)
@@ -162,8 +162,12 @@ __device__ __forceinline__ void flush_far(const float4 *__restrict__ far, int nf
 // itself, or a coincident particle) contributes nothing and is not counted.
 // POT: the potential-only walk, which has no r^2 > 0 condition: an r = 0 pair
 // adds m w_pot(0) / h like any other (the caller removes the self term).
-template <int TPL, bool POT>
-__device__ __forceinline__ void flush_near(const float4 *__restrict__ nearE, const float2 *__restrict__ nearH, int nn,
+// HOMOG: every target of the group has the same kernel radius h_t, so the
+// pair's softening h_g = max(h_t, h_source) and its products are per entry,
+// formed when the entry was listed: nearH = {h_g, 1/h_g, m/h_g, m/h_g^3}.
+// Otherwise nearH = {h_source, 1/h_source} and h_g is formed per pair.
+template <int TPL, bool POT, bool HOMOG>
+__device__ __forceinline__ void flush_near(const float4 *__restrict__ nearE, const float4 *__restrict__ nearH, int nn,
                                            Targets<TPL> &T)
 {
     __syncwarp();
@@ -174,27 +178,25 @@ __device__ __forceinline__ void flush_near(const float4 *__restrict__ nearE, con
 #pragma unroll 2
     for (int j = 0; j < nn; j++) {
         const float4 e = nearE[j];
-        const float2 hh = nearH[j];   // source kernel radius and its inverse
-        const float hp = hh.x;
+        const float4 hh = nearH[j];
 #pragma unroll
         for (int s = 0; s < TPL; s++) {
             const float dx = e.x - T.x[s], dy = e.y - T.y[s], dz = e.z - T.z[s];
             const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            const float hg = fmaxf(T.h[s], hp);
-            const float hinv = fminf(T.hinv[s], hh.y);   // 1/h_g: the inverses are rounded alike
+            const float hg = HOMOG ? hh.x : fmaxf(T.h[s], hh.x);
+            const float hinv = HOMOG ? hh.y : fminf(T.hinv[s], hh.y);   // 1/h_g: the inverses are rounded alike
             const float rinv = rsqrtf(POT ? fmaxf(r2, 1e-30f) : r2);   // finite at r = 0 when it counts
             const float mr = e.w * rinv;
             // spline for r < h_g (kernel.h:452-470), Newtonian beyond (:391-398)
             const float u = r2 * rinv * hinv, iu = hg * rinv;
             float wp;
             const float wf = spline_wf(u, iu, &wp);
-            const float hinv2 = hinv * hinv;
             const bool soft = r2 < hg * hg;
-            float fpot = soft ? e.w * wp * hinv : -mr;
+            float fpot = soft ? (HOMOG ? hh.z * wp : e.w * wp * hinv) : -mr;
             if (POT) {
                 pp[s] += fpot;
             } else {
-                float fac = soft ? e.w * wf * (hinv2 * hinv) : mr * rinv * rinv;
+                float fac = soft ? (HOMOG ? hh.w * wf : e.w * wf * (hinv * hinv * hinv)) : mr * rinv * rinv;
                 const bool use = r2 > 0.f;
                 fac = use ? fac : 0.f;
                 fpot = use ? fpot : 0.f;
@@ -213,6 +215,25 @@ __device__ __forceinline__ void flush_near(const float4 *__restrict__ nearE, con
         T.nint[s] += nn - self[s];
     }
     __syncwarp();
+}
+
+template <int TPL, bool POT>
+__device__ __forceinline__ void flush_near_sel(bool homog, const float4 *__restrict__ nearE,
+                                               const float4 *__restrict__ nearH, int nn, Targets<TPL> &T)
+{
+    if (homog) flush_near<TPL, POT, true>(nearE, nearH, nn, T);
+    else flush_near<TPL, POT, false>(nearE, nearH, nn, T);
+}
+
+// softening record of a near-list entry with kernel radius hsrc and mass m (see flush_near)
+__device__ __forceinline__ float4 near_soft(float hsrc, float m, bool homog, float hgroup)
+{
+    if (homog) {
+        const float hg = fmaxf(hgroup, hsrc);
+        const float hinv = hg > 0.f ? __frcp_rn(hg) : INFINITY;
+        return make_float4(hg, hinv, m * hinv, m * (hinv * hinv * hinv));
+    }
+    return make_float4(hsrc, hsrc > 0.f ? __frcp_rn(hsrc) : INFINITY, 0.f, 0.f);
 }
 
 __device__ __forceinline__ double warp_min_d(double v)
@@ -251,8 +272,8 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
     const int FL = p.flush, cap = FL + 32;
     float4 *far = walk_smem + (size_t)warp * walk_warp_float4s(FL);
     float4 *nearE = far + cap;
-    float2 *nearH = reinterpret_cast<float2 *>(nearE + cap);
-    int *sstack = reinterpret_cast<int *>(far + 2 * cap + (cap + 1) / 2);
+    float4 *nearH = nearE + cap;
+    int *sstack = reinterpret_cast<int *>(far + 3 * cap);
     int *gstack = p.stack + (size_t)(blockIdx.x * WALK_WARPS + warp) * p.stack_cap;
     const int ngroups = *p.ngroups;
     const double theta = p.theta;
@@ -319,6 +340,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
         const double hmaxd = (double)hmax, hmind = (double)hmin;
         const float hwf[3] = {__double2float_ru(hw[0]), __double2float_ru(hw[1]), __double2float_ru(hw[2])};
         const float aoldf = (float)aold_min, thetaf = (float)theta;
+        const bool homog = hmin == hmax;   // one kernel radius in the group (warp-uniform)
 
         // ---- traversal
         // The node stack lives in shared memory (sp entries) on top of a spill
@@ -433,7 +455,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
                     else {
                         int pos = nn + __popc(mn & lt_mask);
                         nearE[pos] = ent;
-                        nearH[pos] = make_float2(hp, hp > 0.f ? __frcp_rn(hp) : INFINITY);
+                        nearH[pos] = near_soft(hp, ent.w, homog, hmax);
                     }
                 }
                 nf += __popc(mf);
@@ -472,7 +494,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
             GGNode nxt;
             if (lane < next_k) nxt = load_node(p.nodes + next_node);
             if (nf >= FL) { flush_far<TPL, POT>(far, nf, T); nf = 0; }
-            if (nn >= FL) { flush_near<TPL, POT>(nearE, nearH, nn, T); nn = 0; }
+            if (nn >= FL) { flush_near_sel<TPL, POT>(homog, nearE, nearH, nn, T); nn = 0; }
             // opened leaves -> particles, 32 at a time
             {
                 int cnt = (act == 3) ? -nb : 0;
@@ -515,7 +537,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
                         else {
                             int pos = nn + __popc(mn & lt_mask);
                             nearE[pos] = pe;
-                            nearH[pos] = make_float2(ph, ph > 0.f ? __frcp_rn(ph) : INFINITY);
+                            nearH[pos] = near_soft(ph, pe.w, homog, hmax);
                         }
                     }
                     nf += __popc(mf);
@@ -523,7 +545,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
                     list_far += __popc(mf);
                     list_near += __popc(mn);
                     if (nf >= FL) { flush_far<TPL, POT>(far, nf, T); nf = 0; }
-                    if (nn >= FL) { flush_near<TPL, POT>(nearE, nearH, nn, T); nn = 0; }
+                    if (nn >= FL) { flush_near_sel<TPL, POT>(homog, nearE, nearH, nn, T); nn = 0; }
                 }
             }
             k = next_k;
@@ -535,7 +557,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
             continue;
         }
         if (nf > 0) flush_far<TPL, POT>(far, nf, T);
-        if (nn > 0) flush_near<TPL, POT>(nearE, nearH, nn, T);
+        if (nn > 0) flush_near_sel<TPL, POT>(homog, nearE, nearH, nn, T);
 
         // ---- results
         int mycount = 0;
