@@ -186,17 +186,24 @@ __device__ __forceinline__ void flush_near(const float4 *__restrict__ nearE, con
             const float hg = HOMOG ? hh.x : fmaxf(T.h[s], hh.x);
             const float hinv = HOMOG ? hh.y : fminf(T.hinv[s], hh.y);   // 1/h_g: the inverses are rounded alike
             const float rinv = rsqrtf(POT ? fmaxf(r2, 1e-30f) : r2);   // finite at r = 0 when it counts
-            const float mr = e.w * rinv;
-            // spline for r < h_g (kernel.h:452-470), Newtonian beyond (:391-398)
+            // spline for u = r/h_g < 1 (kernel.h:452-470), Newtonian beyond (:391-398);
+            // the two meet at u = 1, where the spline's force factor is 1/u^3
             const float u = r2 * rinv * hinv, iu = hg * rinv;
             float wp;
             const float wf = spline_wf(u, iu, &wp);
-            const bool soft = r2 < hg * hg;
-            float fpot = soft ? (HOMOG ? hh.z * wp : e.w * wp * hinv) : -mr;
+            const bool soft = u < 1.f;
+            float fpot, fac = 0.f;
+            if (HOMOG) {   // Newtonian as m/h_g^3 (1/u)^3 and -m/h_g (1/u), on the entry's products
+                fpot = hh.z * (soft ? wp : -iu);
+                if (!POT) fac = hh.w * (soft ? wf : iu * iu * iu);
+            } else {
+                const float mr = e.w * rinv;
+                fpot = soft ? e.w * wp * hinv : -mr;
+                if (!POT) fac = soft ? e.w * wf * (hinv * hinv * hinv) : mr * rinv * rinv;
+            }
             if (POT) {
                 pp[s] += fpot;
             } else {
-                float fac = soft ? (HOMOG ? hh.w * wf : e.w * wf * (hinv * hinv * hinv)) : mr * rinv * rinv;
                 const bool use = r2 > 0.f;
                 fac = use ? fac : 0.f;
                 fpot = use ? fpot : 0.f;
