@@ -1400,3 +1400,9 @@ extern "C" gg_status gg_get_order(gg_ctx *c, int32_t *order_out)
     GG_CUDA_TRY(cudaStreamSynchronize(c->stream));
     return GG_OK;
 }
+
+// ---------------------------------------------------------------- self-test of the bounded waits
+extern "C" gg_status gg_selftest_bounded_wait(void *stream)
+{
+    return gg_sort_timeout_selftest((cudaStream_t)stream);
+}

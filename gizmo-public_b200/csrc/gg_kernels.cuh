@@ -87,3 +87,6 @@ void gg_launch_drift(GGPart *in_rec, GGPart *parts, const unsigned *perm, const 
 // FP64 per-system sums {1/2 sum m phi, sum m a} (gg_util.cu)
 void gg_launch_energy(const int4 *chunks, int nchunks, const int *sys_first_chunk, int S, const GGPart *rec,
                       const double *acc, const double *pot, double *part, double *out, cudaStream_t st);
+
+// bounded look-back self-test (gg_sort.cu)
+gg_status gg_sort_timeout_selftest(cudaStream_t st);

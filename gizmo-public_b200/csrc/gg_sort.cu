@@ -296,3 +296,45 @@ gg_status gg_sort_pairs_run(unsigned long long *keys, unsigned *vals, long long 
     }
     return GG_OK;
 }
+
+// Self-test of the bounded look-back: one CTA runs tile 1 of a two-tile pass
+// whose tile 0 never runs, so its look-back gives up after GG_SORT_SPIN_LIMIT
+// polls and records GG_EBIT_SORT_TIMEOUT.  Every access stays in bounds: the
+// status words and buffers are sized for two tiles and the scatter checks
+// gpos < n.  Returns GG_ERR_TIMEOUT when the limit works, GG_OK if the wait
+// completed (it cannot), or a CUDA error.
+gg_status gg_sort_timeout_selftest(cudaStream_t st)
+{
+    const int n = 2 * SORT_TILE;
+    const size_t bytes = gg_sort_scratch_bytes(n, 1);
+    char *base = nullptr;
+    GG_CUDA_TRY(cudaMallocAsync((void **)&base, bytes + 4 * (size_t)n * 12 + 1024, st));
+    char *p = base;
+    auto take = [&](size_t b) { char *r = p; p += (b + 255) & ~(size_t)255; return (void *)r; };
+    unsigned long long *kin = (unsigned long long *)take((size_t)n * 8);
+    unsigned *vin = (unsigned *)take((size_t)n * 4);
+    unsigned long long *kout = (unsigned long long *)take((size_t)n * 8);
+    unsigned *vout = (unsigned *)take((size_t)n * 4);
+    unsigned *off = (unsigned *)take(RADIX * 4);
+    unsigned *status = (unsigned *)take(2 * RADIX * 4);
+    unsigned *counter = (unsigned *)take(256);
+    int *err = (int *)take(256);
+    cudaMemsetAsync(base, 0, (size_t)(p - base), st);
+    const unsigned one = 1;   // the CTA takes tile 1; tile 0 is never started
+    cudaMemcpyAsync(counter, &one, sizeof one, cudaMemcpyHostToDevice, st);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, sort_smem_bytes());
+        attr_set = true;
+    }
+    k_sort_pass<<<1, SORT_THREADS, sort_smem_bytes(), st>>>(kin, vin, kout, vout, n, 0, 0, nullptr, 1, off, status,
+                                                             counter, err);
+    gg_note_launches(1);
+    int herr = 0;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, err, sizeof herr, cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(base, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return gg_cuda_fail(e);
+    return (herr & GG_EBIT_SORT_TIMEOUT) ? GG_ERR_TIMEOUT : GG_OK;
+}

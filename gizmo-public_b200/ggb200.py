@@ -114,6 +114,7 @@ def load_library():
             "gg_fp32_peak_probe": (i32, [ctypes.POINTER(dbl), P]),
             "gg_radix_sort_pairs_noalloc": (i32, [i64, P, P, i32, P]),
             "gg_kernel_launches": (i64, []),
+            "gg_selftest_bounded_wait": (i32, [P]),
             "gg_load_velocities": (i32, [P, P, i64]),
             "gg_load_velocities_device": (i32, [P, P]),
             "gg_drift": (i32, [P, dbl]),
@@ -451,6 +452,12 @@ def direct_sum_fp64(d_pos, d_mass, d_h, n_src, d_targets, n_tgt, d_acc, d_pot, s
 def reserve_device_pool(nbytes, device=0):
     """Grow the device's memory pool by nbytes once (see gg_reserve_device_pool)."""
     _check(load_library().gg_reserve_device_pool(int(device), int(nbytes)), "gg_reserve_device_pool")
+
+
+def selftest_bounded_wait(stream=None):
+    """Run the sort look-back's bounded-wait self-test; returns the status
+    (GG_ERR_TIMEOUT, -5, is the expected result)."""
+    return int(load_library().gg_selftest_bounded_wait(stream))
 
 
 def fp32_peak_tflops(stream=None):

@@ -259,6 +259,13 @@ gg_status gg_radix_sort_pairs(int64_t n, uint64_t *d_keys, uint32_t *d_vals, int
  * on the GPU race and must not be issued.  Blocking (synchronises `stream`). */
 #define GG_NOALLOC_SORT_MAX_N (1 << 20)
 gg_status gg_radix_sort_pairs_noalloc(int64_t n, uint64_t *d_keys, uint32_t *d_vals, int32_t key_bits, void *stream);
+/* Self-test of the library's only device-side wait, the radix sort's
+ * look-back: one sort pass is run as the second tile of a two-tile pass whose
+ * first tile never runs, so the wait cannot complete.  It gives up after its
+ * poll limit (about a second) and the call returns GG_ERR_TIMEOUT, which is
+ * the expected result; the device stays usable.  No counterpart in the
+ * reference (its sort runs on the host).  Blocking. */
+gg_status gg_selftest_bounded_wait(void *stream);
 /* FP64 direct summation over all sources with the walk's pair rule (the
  * reference declares force_treeevaluate_direct, gravity/forcetree.h:76, but
  * ships no definition); used to measure force errors at full size */

@@ -234,3 +234,20 @@ def test_full_size_galaxy_properties():
     ptot = (ic["mass"][:, None] * acc).sum(0)
     assert np.linalg.norm(ptot) < 1e-3 * (ic["mass"][:, None] * np.abs(acc)).sum()
     assert st["interactions"] == nint.sum()
+
+
+def test_bounded_wait_returns_timeout_and_the_device_stays_usable():
+    """The sort's look-back waits on a predecessor tile; when that tile never
+    runs, the wait gives up after its poll limit and the call reports
+    GG_ERR_TIMEOUT instead of hanging.  The next sort works."""
+    import time
+    torch = torch_cuda()
+    t0 = time.time()
+    assert ggb200.selftest_bounded_wait() == -5      # GG_ERR_TIMEOUT
+    assert time.time() - t0 < 30
+    keys = np.random.default_rng(9).integers(0, 1 << 62, size=10000, dtype=np.uint64)
+    dk = torch.from_numpy(keys.view(np.int64).copy()).cuda()
+    dv = torch.arange(10000, dtype=torch.int32, device="cuda")
+    ggb200.radix_sort_pairs(dk, dv, 10000, 64)
+    torch.cuda.synchronize()
+    assert np.array_equal(dk.cpu().numpy().view(np.uint64), np.sort(keys))
