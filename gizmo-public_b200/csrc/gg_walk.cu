@@ -88,6 +88,14 @@ struct Kahan {
     __device__ __forceinline__ double value() const { return (double)s - (double)c; }
 };
 
+// This file is compiled with denormals flushed to zero (-ftz=true): rsqrtf and
+// the reciprocals are then single hardware approximations without range
+// fix-ups.  An entry goes to the far list only when its squared distance from
+// the group's box exceeds FAR_MIN_R2, so every far pair has a normal r^2; near
+// pairs are selected, not multiplied, out of the sums when r^2 is zero (and
+// r^2 below the smallest normal float is zero here).
+#define FAR_MIN_R2 1e-36f
+
 // Cubic-spline softened force and potential factors for u = r/h < 1
 // (kernel.h:452-470), without a branch or a per-piece coefficient choice.  The
 // outer piece (0.5 <= u < 1) equals the inner polynomial plus a correction
@@ -419,7 +427,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
                             ent = make_float4(dx, dy, dz, nd.mass);
                             hp = ms;
                             const float hh = fmaxf(hmax, ms);
-                            isfar = (r2 >= hh * hh) && (r2 > 0.f);
+                            isfar = (r2 >= hh * hh) && (r2 > FAR_MIN_R2);
                         }
                     } else {
                         double dx = nd.cx - cg[0], dy = nd.cy - cg[1], dz = nd.cz - cg[2];
@@ -448,7 +456,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
                             ent = make_float4((float)dx, (float)dy, (float)dz, nd.mass);
                             hp = nd.maxsoft;
                             double hh = fmax(hmaxd, ms);
-                            isfar = (r2 >= hh * hh) && (r2 > 0.0);
+                            isfar = (r2 >= hh * hh) && (r2 > (double)FAR_MIN_R2);
                         }
                     }
                 }
@@ -534,7 +542,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
                             pe = make_float4(dx, dy, dz, pp.m);
                             ph = pp.h;
                             use = true;
-                            pfar = (r2 >= hh * hh) && (r2 > 0.f);
+                            pfar = (r2 >= hh * hh) && (r2 > FAR_MIN_R2);
                         }
                     }
                     unsigned mf = __ballot_sync(FULL, use && pfar);
