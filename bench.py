@@ -270,7 +270,7 @@ def run_ensemble(args, torch, ggb200, dist, world, rank, local):
     tol = args.tol
 
     tree = ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush, device=local,
-                              blocks_per_sm=args.blocks_per_sm)
+                              blocks_per_sm=args.blocks_per_sm, group_order=args.group_order)
     tree.set_stream(stream.cuda_stream)
     tree.load_device(d_rec, counts)
     tree.build()
@@ -332,7 +332,7 @@ def run_ensemble(args, torch, ggb200, dist, world, rank, local):
     d_acc_p = torch.empty((n, 3), dtype=torch.float64, device=dev)
     d_pot_p = torch.empty(n, dtype=torch.float64, device=dev)
     plain = ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush, device=local,
-                               blocks_per_sm=args.blocks_per_sm)
+                               blocks_per_sm=args.blocks_per_sm, group_order=args.group_order)
     plain.set_stream(stream.cuda_stream)
 
     def plain_pass():
@@ -558,7 +558,8 @@ def run_split(args, torch, ggb200, dist, world, rank, local):
     d_acc = torch.empty((share[rank], 3), dtype=torch.float64, device=dev)
     d_pot = torch.empty(share[rank], dtype=torch.float64, device=dev)
     tree = ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush, device=local,
-                              blocks_per_sm=args.blocks_per_sm, target_order=args.target_order)
+                              blocks_per_sm=args.blocks_per_sm, target_order=args.target_order,
+                              group_order=args.group_order)
     tree.set_stream(stream.cuda_stream)
     split = multi.SplitSystem(dist, tree, torch, dev)
     split.step(d_rec, d_acc, d_pot, err_tol_theta=0.7)
@@ -660,6 +661,8 @@ def main():
     ap.add_argument("--flush", type=int, default=64)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--target-order", type=int, default=1, choices=[0, 1])
+    ap.add_argument("--group-order", type=int, default=1, choices=[0, 1],
+                    help="1: walk groups handed out most expensive first, by the previous walk's costs")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--serve-window", type=float, default=2.0)
     # individual timesteps: the timed walk evaluates a seeded random fraction of
@@ -704,7 +707,7 @@ def main():
 
     tree = ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush,
                               device=local, blocks_per_sm=args.blocks_per_sm,
-                              target_order=args.target_order)
+                              target_order=args.target_order, group_order=args.group_order)
     tree.set_stream(stream.cuda_stream)
     tree.load_device(d_rec, [n])
     # start-up Barnes-Hut pass gives OldAcc (accel.c:47-50), left on the device
@@ -770,14 +773,16 @@ def main():
 
     # stage breakdown on one extra instrumented step (outside the timed region)
     tprof = ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush, device=local,
-                               timing=True, blocks_per_sm=args.blocks_per_sm, target_order=args.target_order)
+                               timing=True, blocks_per_sm=args.blocks_per_sm, target_order=args.target_order,
+                              group_order=args.group_order)
     tprof.set_stream(stream.cuda_stream)
     tprof.load_device(d_rec, [n])
     tprof.build()
     tprof.evaluate_device(d_acc, d_pot, err_tol_theta=0.7)
-    if act is not None:
-        tprof.build()
-        tprof.evaluate_device(d_acc, d_pot, err_tol_force_acc=args.tol, err_tol_theta=0.0)
+    # one relative walk first, so that the measured step starts, like the timed
+    # steps, from a relative walk's OldAcc and group costs
+    tprof.build()
+    tprof.evaluate_device(d_acc, d_pot, err_tol_force_acc=args.tol, err_tol_theta=0.0)
     tprof.build()
     walk(tprof)
     stages = tprof.last_stats()
@@ -831,7 +836,7 @@ def main():
             old = torch.linalg.norm(d_acc, dim=1).cpu().numpy()
         with ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush,
                                 device=local, blocks_per_sm=args.blocks_per_sm,
-                              target_order=args.target_order) as te:
+                              target_order=args.target_order, group_order=args.group_order) as te:
             out = (np.empty((na, 3)), np.empty(na))   # the caller's result arrays, reused every step
 
             def e2e_step():
@@ -866,6 +871,7 @@ def main():
                    "step": "extent+keys+sort+permute+tree+moments+relative walk (OldAcc on device)",
                    "l2": "inputs larger than L2 (32 B/particle records, 134 MB + tree)",
                    "leaf_size": args.leaf, "group_size": args.group, "flush": args.flush,
+                   "group_order": "by previous walk's cost" if args.group_order else "target order",
                    "parallelism": "independent system per GPU" if world > 1 else "1 GPU"},
         "force_error": {"p50": p50, "p99": p99, "targets": ne, "vs": "FP64 direct sum (GPU, same pair rule)",
                         "pot_sum_rel_diff_sample": abs(wsum - wsum_dir) / abs(wsum_dir)},

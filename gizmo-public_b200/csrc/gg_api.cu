@@ -223,6 +223,12 @@ struct gg_ctx {
     DevBuf<int> e_first;
     DevBuf<double> e_part, e_out;
     bool oldacc_valid = false;
+    // group order by measured cost: per target (load order) the previous walk's
+    // group cycles per target, and the sorted group order
+    DevBuf<float> tcost;
+    bool tcost_valid = false;
+    DevBuf<unsigned long long> gkey;
+    DevBuf<unsigned> gorder;
     DevBuf<GGGroup> groups;
     DevBuf<int> ngroups, gscan, toff, flag, flagscan, tlist, tout, scan_scratch, active_d;
     DevBuf<int> counters;                  // [0] group counter
@@ -260,7 +266,7 @@ struct gg_ctx {
         f(keys); f(perm); f(rank); f(sort_scratch);
         f(t_start); f(t_end); f(t_level); f(t_parent); f(t_sys); f(t_nch); f(t_child); f(t_counter); f(t_bnd);
         f(t_depth); f(t_nnodes); f(t_bsum); f(t_boff); f(t_mass64); f(nodes);
-        f(oldacc); f(vel); f(kin); f(kin_counter); f(dts); f(oldacc_save);
+        f(oldacc); f(vel); f(kin); f(kin_counter); f(dts); f(oldacc_save); f(tcost); f(gkey); f(gorder);
         f(e_chunks); f(e_first); f(e_part); f(e_out);
         f(groups); f(ngroups); f(gscan); f(toff); f(flag); f(flagscan); f(tlist); f(tout); f(scan_scratch);
         f(active_d); f(counters); f(inter); f(stack); f(err); f(acc_d); f(pot_d); f(nint_d);
@@ -291,6 +297,7 @@ extern "C" void gg_config_default(gg_config *cfg)
     cfg->walk_blocks_per_sm = 0;
     cfg->timing = 0;
     cfg->target_order = 1;
+    cfg->group_order = 1;
 }
 
 extern "C" const char *gg_strerror(gg_status s)
@@ -337,6 +344,7 @@ extern "C" gg_status gg_create(const gg_config *cfg, gg_ctx **out)
     if (c.leaf_size < 1 || c.leaf_size > 32) return GG_ERR_INVALID;
     if (c.group_size < 1 || c.group_size > 64) return GG_ERR_INVALID;
     if (c.flush_threshold < 32 || c.flush_threshold > 128) return GG_ERR_INVALID;
+    if (c.group_order != 0 && c.group_order != 1) return GG_ERR_INVALID;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= c.device || c.device < 0) {
         cudaGetLastError();
@@ -439,6 +447,7 @@ static gg_status set_systems(gg_ctx *c, int S, const int64_t *counts)
         if (N >= (1ll << 30)) return GG_ERR_TOO_LARGE;
     }
     poff[S] = (int)N;
+    if (N != c->N || S != c->S) c->tcost_valid = false;   // same particles reloaded keep their costs
     c->S = S;
     c->N = N;
     c->h_poff = poff;
@@ -622,6 +631,10 @@ static gg_status walk_setup(gg_ctx *c)
         (st = c->stack.ensure((size_t)c->walk_blocks * gg_num_sms() * (gg_walk_threads() / 32) * GG_STACK_CAP)) ||
         (st = c->scan_scratch.ensure(gg_scan_scratch_ints())))
         return st;
+    if (c->cfg.group_order &&
+        ((st = c->tcost.ensure(c->N + 1)) || (st = c->gkey.ensure(maxg)) || (st = c->gorder.ensure(maxg)) ||
+         (st = c->sort_scratch.ensure(gg_sort_scratch_bytes(maxg, 1)))))
+        return st;
     return GG_OK;
 }
 
@@ -663,6 +676,16 @@ static gg_status run_walk(gg_ctx *c, const int *d_active, int n_active, const do
         c->oldacc_valid = true;
     }
     gg_launch_groups(toff, S, c->cfg.group_size, c->groups.p, c->ngroups.p, c->gscan.p, s);
+    const unsigned *gorder = nullptr;
+    if (c->cfg.group_order && !c->tcost_valid)   // a fresh history: targets not walked yet cost 0
+        GG_CUDA_TRY(cudaMemsetAsync(c->tcost.p, 0, (size_t)c->N * sizeof(float), s));
+    if (c->cfg.group_order && c->tcost_valid) {
+        const long long maxg = c->N / c->cfg.group_size + c->S + 1;
+        if ((st = gg_order_groups_by_cost(c->groups.p, c->ngroups.p, (int)maxg, tlist, c->perm.p, c->tcost.p,
+                                          c->gkey.p, c->gorder.p, c->sort_scratch.p, c->err.p, s)))
+            return st;
+        gorder = c->gorder.p;
+    }
     GG_CUDA_TRY(cudaMemsetAsync(c->counters.p, 0, 8 * sizeof(int), s));
     GG_CUDA_TRY(cudaMemsetAsync(c->inter.p, 0, 4 * sizeof(unsigned long long), s));
     WalkParams p;
@@ -689,11 +712,14 @@ static gg_status run_walk(gg_ctx *c, const int *d_active, int n_active, const do
     p.flush = c->cfg.flush_threshold;
     p.pot_only = pot_only ? 1 : 0;
     if (pot_only) p.acc = nullptr;
+    p.gorder = gorder;
+    p.cost_out = c->cfg.group_order ? c->tcost.p : nullptr;
     int tpl = c->cfg.group_size > 32 ? 2 : 1;
     if (c->cfg.timing) cudaEventRecord(c->ev[4], s);
     gg_launch_walk(p, tpl, c->walk_blocks, s);
     if (c->cfg.timing) cudaEventRecord(c->ev[5], s);
     if (!pot_only) c->oldacc_valid = true;
+    if (c->cfg.group_order) c->tcost_valid = true;
     GG_CUDA_TRY(cudaGetLastError());
     return GG_OK;
 }

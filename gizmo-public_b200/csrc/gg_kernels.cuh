@@ -53,6 +53,8 @@ struct WalkParams {
     int group_size;
     int flush;
     int pot_only;               // potential-only walk: acc and oldacc_out unused, pot required
+    const unsigned *gorder;     // order in which groups are handed out, NULL = index order
+    float *cost_out;            // per particle (load order): its group's cycles per target, may be NULL
 };
 int gg_walk_smem_bytes(int flush, int tpl);
 void gg_launch_walk(const WalkParams &p, int tpl, int blocks_per_sm, cudaStream_t st);
@@ -67,6 +69,11 @@ void gg_launch_active(const int *active, int n_active, const unsigned *rank, int
                       int *tlist, int *tout, const int *poff, int S, int *toff, int *scratch, int *err,
                       cudaStream_t st);
 int gg_scan_scratch_ints();
+// walk groups sorted by the summed previous cost of their targets, most
+// expensive first: gorder[0..maxg) (groups past the device count sort last)
+gg_status gg_order_groups_by_cost(const GGGroup *groups, const int *ngroups, int maxg, const int *tlist,
+                                  const unsigned *perm, const float *cost, unsigned long long *key,
+                                  unsigned *gorder, void *sort_scratch, int *err, cudaStream_t st);
 // targets reordered by (system, kernel radius), key order kept within a class
 gg_status gg_order_targets_by_softening(int nt, const int *tlist_in, const int *tout_in, const GGPart *parts,
                                         const unsigned long long *pkeys, const int *poff, int S,

@@ -148,6 +148,50 @@ void gg_launch_groups(const int *toff, int S, int gs, GGGroup *groups, int *ngro
     gg_note_launches(2);
 }
 
+// ---- group order by measured cost -----------------------------------------------
+// Groups are handed to the persistent walk warps by an atomic counter.  In
+// target order the dearest groups (dense centres, sparse outskirts) may come
+// last and leave a tail in which few warps still work.  Each walk records per
+// target its group's device cycles divided by the group's size; the next walk
+// sums these over each of its own groups and hands the groups out most
+// expensive first (longest-processing-time-first list scheduling), by whole
+// octaves of cost: that ends the walk as early as a full sort by cost would
+// on the measured galaxy, clustered and Plummer costs, and keeps most groups
+// in target order.  A group's result does not depend on when it runs, so the
+// order changes no output.
+__global__ void k_group_cost(const GGGroup *__restrict__ groups, const int *__restrict__ ngroups, int maxg,
+                             const int *__restrict__ tlist, const unsigned *__restrict__ perm,
+                             const float *__restrict__ cost, unsigned long long *key, unsigned *val)
+{
+    const int ng = *ngroups;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < maxg; g += gridDim.x * blockDim.x) {
+        unsigned k = 255u;   // past the device count: last
+        if (g < ng) {
+            const GGGroup G = groups[g];
+            float c = 0.f;
+            for (int t = G.first; t < G.first + G.count; t++) c += cost[perm[tlist ? tlist[t] : t]];
+            // descending octave of the cost (the float's exponent field); a
+            // valid group never takes the last key
+            k = 255u - max(__float_as_uint(fmaxf(c, 0.f)) >> 23, 1u);
+        }
+        key[g] = k;
+        val[g] = (unsigned)g;
+    }
+}
+
+gg_status gg_order_groups_by_cost(const GGGroup *groups, const int *ngroups, int maxg, const int *tlist,
+                                  const unsigned *perm, const float *cost, unsigned long long *key,
+                                  unsigned *gorder, void *sort_scratch, int *err, cudaStream_t st)
+{
+    if (maxg <= 0) return GG_OK;
+    const int blocks = std::max(1, std::min(gg_num_sms() * 4, (maxg + 255) / 256));
+    k_group_cost<<<blocks, 256, 0, st>>>(groups, ngroups, maxg, tlist, perm, cost, key, gorder);
+    gg_note_launches(1);
+    // one 8-bit pass; the sort is stable, so the groups of one cost octave keep
+    // target order and neighbouring warps still walk neighbouring regions
+    return gg_sort_pairs_run(key, gorder, maxg, 1, 0, nullptr, 1, sort_scratch, err, st);
+}
+
 // ---- active targets ------------------------------------------------------------
 __global__ void k_mark_active(const int *__restrict__ active, int n_active, const unsigned *__restrict__ rank, int n,
                               int *flag, int *err)

@@ -298,7 +298,8 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
         if (lane == 0) g = atomicAdd(p.group_counter, 1);
         g = __shfl_sync(FULL, g, 0);
         if (g >= ngroups) break;
-        const GGGroup grp = p.groups[g];
+        const GGGroup grp = p.groups[p.gorder ? (int)p.gorder[g] : g];
+        const long long t_start = clock64();
 
         // ---- targets of the group
         Targets<TPL> T;
@@ -575,6 +576,8 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
         if (nn > 0) flush_near_sel<TPL, POT>(homog, nearE, nearH, nn, T);
 
         // ---- results
+        // this group's device cycles per target: the cost the next walk orders its groups by
+        const float tcost = (float)(clock64() - t_start) / (float)grp.count;
         int mycount = 0;
 #pragma unroll
         for (int s = 0; s < TPL; s++) {
@@ -597,6 +600,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
                 if (p.oldacc_out) p.oldacc_out[li] = sqrt(ax * ax + ay * ay + az * az);
             }
             if (p.ninter) p.ninter[o] = T.nint[s];
+            if (p.cost_out) p.cost_out[li] = tcost;
             mycount += T.nint[s];
         }
 #pragma unroll

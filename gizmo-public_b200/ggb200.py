@@ -49,7 +49,7 @@ class GravityError(RuntimeError):
 class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("leaf_size", ctypes.c_int32), ("group_size", ctypes.c_int32),
                 ("flush_threshold", ctypes.c_int32), ("walk_blocks_per_sm", ctypes.c_int32),
-                ("timing", ctypes.c_int32), ("target_order", ctypes.c_int32), ("reserved", ctypes.c_int32 * 1)]
+                ("timing", ctypes.c_int32), ("target_order", ctypes.c_int32), ("group_order", ctypes.c_int32)]
 
 
 class Domain(ctypes.Structure):
@@ -172,7 +172,8 @@ def domain_to_dict(d):
 class GravityTree:
     """One library context: particles of one or more systems, their trees, walks."""
 
-    def __init__(self, leaf_size=8, group_size=32, flush=64, device=0, timing=False, blocks_per_sm=0, target_order=1):
+    def __init__(self, leaf_size=8, group_size=32, flush=64, device=0, timing=False, blocks_per_sm=0, target_order=1,
+                 group_order=1):
         lib = load_library()
         cfg = Config()
         lib.gg_config_default(ctypes.byref(cfg))
@@ -180,6 +181,7 @@ class GravityTree:
         cfg.timing = 1 if timing else 0
         cfg.walk_blocks_per_sm = blocks_per_sm
         cfg.target_order = target_order
+        cfg.group_order = group_order
         h = ctypes.c_void_p()
         _check(lib.gg_create(ctypes.byref(cfg), ctypes.byref(h)), "gg_create")
         self._lib, self._h = lib, h

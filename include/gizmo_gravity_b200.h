@@ -60,7 +60,10 @@ typedef struct gg_config {
                                  targets are ordered by Peano-Hilbert cell at the softening
                                  scale, then by radius, so groups are compact and of one radius
                                  where they can be; 0: plain key order */
-    int32_t reserved[1];
+    int32_t group_order;      /* 1 (default): walk groups are handed out most expensive first, by
+                                 the cost each target had in the previous walk of this context
+                                 (its group's device cycles per target); 0: in target order.
+                                 The order changes no result, only when each group runs */
 } gg_config;
 
 /* root cube of one system: domain_findExtent (domain.c:2518-2570) */
