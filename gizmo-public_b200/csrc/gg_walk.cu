@@ -40,14 +40,14 @@ int gg_walk_threads() { return WALK_THREADS; }
 
 // Per-warp shared memory, in float4 units:
 //   far list float4[cap] | near list float4[cap] | near softening float4[cap] |
-//   node stack int[WALK_SSTACK]
+//   node stack int[WALK_SSTACK] | node slots GGNode[32]
 // with cap = flush + 32.  The stack spills to the warp's global stack area
 // when it overflows (deep or wide traversals only).
 #define WALK_SSTACK 512
 __host__ __device__ __forceinline__ int walk_warp_float4s(int flush)
 {
     const int cap = flush + 32;
-    return 3 * cap + WALK_SSTACK / 4;
+    return 3 * cap + WALK_SSTACK / 4 + 32 * 4;
 }
 
 int gg_walk_smem_bytes(int flush, int tpl)
@@ -56,13 +56,26 @@ int gg_walk_smem_bytes(int flush, int tpl)
     return WALK_WARPS * walk_warp_float4s(flush) * 16;
 }
 
-__device__ __forceinline__ GGNode load_node(const GGNode *p)
+// The next round's node records are staged in shared memory with cp.async, one
+// 64-byte slot per lane, so no registers are held while the loads are in
+// flight (the walk then fits 3 blocks per SM).  A lane refills its slot only
+// after its test of the node in it is complete.
+__device__ __forceinline__ void stage_node(int4 *slot, const GGNode *src)
 {
-    GGNode r;
-    const int4 *src = reinterpret_cast<const int4 *>(p);
-    int4 *dst = reinterpret_cast<int4 *>(&r);
+    const unsigned d = (unsigned)__cvta_generic_to_shared(slot);
+    const int4 *s = reinterpret_cast<const int4 *>(src);
 #pragma unroll
-    for (int i = 0; i < 4; i++) dst[i] = __ldg(src + i);
+    for (int i = 0; i < 4; i++)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d + 16 * i), "l"(s + i) : "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ GGNode staged_node(const int4 *slot)
+{
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    GGNode r;
+    int4 *d = reinterpret_cast<int4 *>(&r);
+#pragma unroll
+    for (int i = 0; i < 4; i++) d[i] = slot[i];
     return r;
 }
 
@@ -289,6 +302,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
     float4 *nearE = far + cap;
     float4 *nearH = nearE + cap;
     int *sstack = reinterpret_cast<int *>(far + 3 * cap);
+    int4 *nslot = reinterpret_cast<int4 *>(far + 3 * cap + WALK_SSTACK / 4) + 4 * lane;
     int *gstack = p.stack + (size_t)(blockIdx.x * WALK_WARPS + warp) * p.stack_cap;
     const int ngroups = *p.ngroups;
     const double theta = p.theta;
@@ -361,10 +375,11 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
         // ---- traversal
         // The node stack lives in shared memory (sp entries) on top of a spill
         // area in global memory (gsp entries).  Each round pops up to 32 nodes;
-        // the next round's node records are loaded before this round's leaf
-        // particles and list flushes are processed, which hides their latency.
+        // the next round's node records are staged (cp.async) before this
+        // round's leaf particles and list flushes are processed, which hides
+        // their latency.
         int sp = 1, gsp = 0, nf = 0, nn = 0;
-        long long list_far = 0, list_near = 0, tested = 0;   // warp-uniform statistics
+        int list_far = 0, list_near = 0, tested = 0;   // warp-uniform statistics of this group
         bool overflow = false;
         if (lane == 0) sstack[0] = grp.root;
         __syncwarp();
@@ -386,8 +401,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
         };
         int node = -1;
         int k = pop_nodes(node);
-        GGNode cur;
-        if (lane < k) cur = load_node(p.nodes + node);
+        if (lane < k) stage_node(nslot, p.nodes + node);
         while (k > 0) {
             tested += k;
 
@@ -396,7 +410,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
             float4 ent = make_float4(0.f, 0.f, 0.f, 0.f);
             float hp = 0.f;
             if (lane < k) {
-                const GGNode nd = cur;
+                const GGNode nd = staged_node(nslot);
                 na = nd.a;
                 nb = nd.b;
                 if (nd.mass > 0.f) {
@@ -503,12 +517,11 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
                 sp += total;
                 __syncwarp();
             }
-            // next round's node records are loaded now; the loads complete behind
+            // next round's node records are staged now; the copies complete behind
             // this round's flushes and leaf particles
             int next_node = -1;
             const int next_k = pop_nodes(next_node);
-            GGNode nxt;
-            if (lane < next_k) nxt = load_node(p.nodes + next_node);
+            if (lane < next_k) stage_node(nslot, p.nodes + next_node);
             if (nf >= FL) { flush_far<TPL, POT>(far, nf, T); nf = 0; }
             if (nn >= FL) { flush_near_sel<TPL, POT>(homog, nearE, nearH, nn, T); nn = 0; }
             // opened leaves -> particles, 32 at a time
@@ -566,7 +579,6 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
             }
             k = next_k;
             node = next_node;
-            cur = nxt;
         }
         if (overflow) {
             if (lane == 0) atomicOr(p.err, GG_EBIT_STACK_OVERFLOW);
