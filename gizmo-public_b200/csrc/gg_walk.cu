@@ -41,12 +41,15 @@ int gg_walk_threads() { return WALK_THREADS; }
 // Per-warp shared memory, in float4 units:
 //   far list float4[cap] | near list float4[cap] | near softening float4[cap] |
 //   node stack int[WALK_SSTACK] | node slots GGNode[32]
-// with cap = flush + 32.  The stack spills to the warp's global stack area
+// with cap = list_cap(flush) entries of 4 floats.  The stack spills to the warp's global stack area
 // when it overflows (deep or wide traversals only).
 #define WALK_SSTACK 512
+// list capacity in entries: a flush threshold plus one ballot's worth, even
+// (the lists are stored in pairs)
+__host__ __device__ __forceinline__ int list_cap(int flush) { return (flush + 33) & ~1; }
 __host__ __device__ __forceinline__ int walk_warp_float4s(int flush)
 {
-    const int cap = flush + 32;
+    const int cap = list_cap(flush);
     return 3 * cap + WALK_SSTACK / 4 + 32 * 4;
 }
 
@@ -109,6 +112,33 @@ struct Kahan {
 // r^2 below the smallest normal float is zero here).
 #define FAR_MIN_R2 1e-36f
 
+// ---- packed FP32x2 arithmetic (sm_100): one instruction, two IEEE FP32
+// operations with round-to-nearest, each exactly the scalar operation
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 sel2(bool px, bool py, float2 a, float2 b)
+{
+    return make_float2(px ? a.x : b.x, py ? a.y : b.y);
+}
+
+// Interaction lists are stored pair-interleaved: entries 2p and 2p+1 occupy
+// the eight floats {x0, x1, y0, y1, z0, z1, w0, w1} (w: mass), so that one
+// 128-bit shared-memory load gives the register pairs the packed instructions
+// take.  The softening records of the near list use the same layout.
+__device__ __forceinline__ void list_put(float *list, int j, float4 v)
+{
+    float *b = list + ((j >> 1) << 3) + (j & 1);
+    b[0] = v.x;
+    b[2] = v.y;
+    b[4] = v.z;
+    b[6] = v.w;
+}
+// A list of odd length is evaluated with one more entry: massless and 1e18 away
+// (its r^2 is finite and its terms are exactly zero).  The lists have room.
+#define PAD_ENTRY make_float4(1e18f, 1e18f, 1e18f, 0.f)
+
 // Cubic-spline softened force and potential factors for u = r/h < 1
 // (kernel.h:452-470), without a branch or a per-piece coefficient choice.  The
 // outer piece (0.5 <= u < 1) equals the inner polynomial plus a correction
@@ -120,16 +150,18 @@ struct Kahan {
 // iu = 1/u is passed in (the caller has it from r^-1).  The corrections are
 // multiplied out starting from t, so a zero t stays zero however large iu is.
 // Returns w_force, writes w_pot; they are still to be scaled by h^-3 and h^-1.
-__device__ __forceinline__ float spline_wf(float u, float iu, float *wp)
+// Two pairs at a time, in packed FP32x2.
+__device__ __forceinline__ float2 spline_wf2(float2 u, float2 iu, float2 *wp)
 {
-    const float u2 = u * u;
-    const float t = fmaxf(u - 0.5f, 0.f);
-    const float t2 = t * t, t4 = t2 * t2;
-    const float fin = fmaf(u2, fmaf(u, 32.f, -38.4f), 10.666666666667f);
-    const float q = t4 * fmaf(t, fmaf(t, 0.166666666667f, 0.2f), 0.0625f);
-    const float pin = fmaf(u2, fmaf(u2, fmaf(u, 6.4f, -9.6f), 5.333333333333f), -2.8f);
-    *wp = fmaf((t4 * t) * fmaf(t, -8.533333333333f, -6.4f), iu, pin);
-    return fmaf(-256.f, ((q * iu) * iu) * iu, fin);
+    const float2 u2 = mul2(u, u);
+    const float2 um = add2(u, dup2(-0.5f));
+    const float2 t = make_float2(fmaxf(um.x, 0.f), fmaxf(um.y, 0.f));
+    const float2 t2 = mul2(t, t), t4 = mul2(t2, t2);
+    const float2 fin = fma2(u2, fma2(u, dup2(32.f), dup2(-38.4f)), dup2(10.666666666667f));
+    const float2 q = mul2(t4, fma2(t, fma2(t, dup2(0.166666666667f), dup2(0.2f)), dup2(0.0625f)));
+    const float2 pin = fma2(u2, fma2(u2, fma2(u, dup2(6.4f), dup2(-9.6f)), dup2(5.333333333333f)), dup2(-2.8f));
+    *wp = fma2(mul2(mul2(t4, t), fma2(t, dup2(-8.533333333333f), dup2(-6.4f))), iu, pin);
+    return fma2(dup2(-256.f), mul2(mul2(mul2(q, iu), iu), iu), fin);
 }
 
 template <int TPL>
@@ -140,36 +172,51 @@ struct Targets {
     int nint[TPL];
 };
 
+// Far list: Newtonian for every target of the group, two entries per packed
+// instruction.  Each flush keeps one partial sum per entry parity and adds
+// both into the Kahan totals.
 // POT: the potential-only walk (force_treeevaluate_potential, forcetree.c:3169-3474)
 template <int TPL, bool POT>
-__device__ __forceinline__ void flush_far(const float4 *__restrict__ far, int nf, Targets<TPL> &T)
+__device__ __forceinline__ void flush_far(float *__restrict__ far, int nf, Targets<TPL> &T)
 {
+    if ((nf & 1) && (threadIdx.x & 31) == 0) list_put(far, nf, PAD_ENTRY);
     __syncwarp();
-    float px[TPL], py[TPL], pz[TPL], pp[TPL];
+    const float4 *L = reinterpret_cast<const float4 *>(far);
+    float2 px[TPL], py[TPL], pz[TPL], pp[TPL], nx[TPL], ny[TPL], nz[TPL];
 #pragma unroll
-    for (int s = 0; s < TPL; s++) { px[s] = 0.f; py[s] = 0.f; pz[s] = 0.f; pp[s] = 0.f; }
-#pragma unroll 4
-    for (int j = 0; j < nf; j++) {
-        const float4 e = far[j];
+    for (int s = 0; s < TPL; s++) {
+        px[s] = py[s] = pz[s] = pp[s] = dup2(0.f);
+        nx[s] = dup2(-T.x[s]); ny[s] = dup2(-T.y[s]); nz[s] = dup2(-T.z[s]);
+    }
+    const int np = (nf + 1) >> 1;
+#pragma unroll 2
+    for (int q = 0; q < np; q++) {
+        const float4 A = L[2 * q], B = L[2 * q + 1];
+        const float2 ex = make_float2(A.x, A.y), ey = make_float2(A.z, A.w);
+        const float2 ez = make_float2(B.x, B.y), em = make_float2(B.z, B.w);
 #pragma unroll
         for (int s = 0; s < TPL; s++) {
-            float dx = e.x - T.x[s], dy = e.y - T.y[s], dz = e.z - T.z[s];
-            float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            float rinv = rsqrtf(r2);
-            float mr = e.w * rinv;
+            const float2 dx = add2(ex, nx[s]), dy = add2(ey, ny[s]), dz = add2(ez, nz[s]);
+            const float2 r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
+            const float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+            const float2 mr = mul2(em, rinv);
             if (!POT) {
-                float fac = mr * rinv * rinv;
-                px[s] = fmaf(dx, fac, px[s]);
-                py[s] = fmaf(dy, fac, py[s]);
-                pz[s] = fmaf(dz, fac, pz[s]);
+                const float2 fac = mul2(mul2(mr, rinv), rinv);
+                px[s] = fma2(dx, fac, px[s]);
+                py[s] = fma2(dy, fac, py[s]);
+                pz[s] = fma2(dz, fac, pz[s]);
             }
-            pp[s] -= mr;
+            pp[s] = fma2(mr, dup2(-1.f), pp[s]);
         }
     }
 #pragma unroll
     for (int s = 0; s < TPL; s++) {
-        if (!POT) { T.ax[s].add(px[s]); T.ay[s].add(py[s]); T.az[s].add(pz[s]); }
-        T.pot[s].add(pp[s]);
+        if (!POT) {
+            T.ax[s].add(px[s].x + px[s].y);
+            T.ay[s].add(py[s].x + py[s].y);
+            T.az[s].add(pz[s].x + pz[s].y);
+        }
+        T.pot[s].add(pp[s].x + pp[s].y);
         T.nint[s] += nf;
     }
     __syncwarp();
@@ -178,9 +225,9 @@ __device__ __forceinline__ void flush_far(const float4 *__restrict__ far, int nf
 // Near list: entries within the softening of some target of the group.  Most
 // of them need the spline for some lanes and the Newtonian form for others
 // (both for 85% of entries on the galaxy), so every lane evaluates both
-// branch-free and selects; without a branch the loop unrolls over entries and
-// independent entries overlap their dependency chains.  r^2 = 0 (the target
-// itself, or a coincident particle) contributes nothing and is not counted.
+// branch-free and selects, two entries per packed instruction.  r^2 = 0 (the
+// target itself, or a coincident particle) contributes nothing and is not
+// counted.
 // POT: the potential-only walk, which has no r^2 > 0 condition: an r = 0 pair
 // adds m w_pot(0) / h like any other (the caller removes the self term).
 // HOMOG: every target of the group has the same kernel radius h_t, so the
@@ -188,66 +235,88 @@ __device__ __forceinline__ void flush_far(const float4 *__restrict__ far, int nf
 // formed when the entry was listed: nearH = {h_g, 1/h_g, m/h_g, m/h_g^3}.
 // Otherwise nearH = {h_source, 1/h_source} and h_g is formed per pair.
 template <int TPL, bool POT, bool HOMOG>
-__device__ __forceinline__ void flush_near(const float4 *__restrict__ nearE, const float4 *__restrict__ nearH, int nn,
+__device__ __forceinline__ void flush_near(float *__restrict__ nearE, float *__restrict__ nearH, int nn,
                                            Targets<TPL> &T)
 {
+    if ((nn & 1) && (threadIdx.x & 31) == 0) {
+        list_put(nearE, nn, PAD_ENTRY);
+        list_put(nearH, nn, make_float4(1.f, 1.f, 0.f, 0.f));
+    }
     __syncwarp();
-    float px[TPL], py[TPL], pz[TPL], pp[TPL];
+    const float4 *LE = reinterpret_cast<const float4 *>(nearE);
+    const float4 *LH = reinterpret_cast<const float4 *>(nearH);
+    float2 px[TPL], py[TPL], pz[TPL], pp[TPL], nx[TPL], ny[TPL], nz[TPL];
     int self[TPL];
 #pragma unroll
-    for (int s = 0; s < TPL; s++) { px[s] = 0.f; py[s] = 0.f; pz[s] = 0.f; pp[s] = 0.f; self[s] = 0; }
+    for (int s = 0; s < TPL; s++) {
+        px[s] = py[s] = pz[s] = pp[s] = dup2(0.f);
+        nx[s] = dup2(-T.x[s]); ny[s] = dup2(-T.y[s]); nz[s] = dup2(-T.z[s]);
+        self[s] = 0;
+    }
+    const int np = (nn + 1) >> 1;
 #pragma unroll 2
-    for (int j = 0; j < nn; j++) {
-        const float4 e = nearE[j];
-        const float4 hh = nearH[j];
+    for (int q = 0; q < np; q++) {
+        const float4 A = LE[2 * q], B = LE[2 * q + 1], C = LH[2 * q], D = LH[2 * q + 1];
+        const float2 ex = make_float2(A.x, A.y), ey = make_float2(A.z, A.w);
+        const float2 ez = make_float2(B.x, B.y), em = make_float2(B.z, B.w);
+        const float2 hs = make_float2(C.x, C.y), hsinv = make_float2(C.z, C.w);
+        const float2 mh = make_float2(D.x, D.y), mh3 = make_float2(D.z, D.w);
 #pragma unroll
         for (int s = 0; s < TPL; s++) {
-            const float dx = e.x - T.x[s], dy = e.y - T.y[s], dz = e.z - T.z[s];
-            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            const float hg = HOMOG ? hh.x : fmaxf(T.h[s], hh.x);
-            const float hinv = HOMOG ? hh.y : fminf(T.hinv[s], hh.y);   // 1/h_g: the inverses are rounded alike
-            const float rinv = rsqrtf(POT ? fmaxf(r2, 1e-30f) : r2);   // finite at r = 0 when it counts
+            const float2 dx = add2(ex, nx[s]), dy = add2(ey, ny[s]), dz = add2(ez, nz[s]);
+            const float2 r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
+            const float2 hg = HOMOG ? hs : make_float2(fmaxf(T.h[s], hs.x), fmaxf(T.h[s], hs.y));
+            // 1/h_g: the inverses are rounded alike
+            const float2 hinv = HOMOG ? hsinv : make_float2(fminf(T.hinv[s], hsinv.x), fminf(T.hinv[s], hsinv.y));
+            // finite at r = 0 when it counts
+            const float2 rinv = make_float2(rsqrtf(POT ? fmaxf(r2.x, 1e-30f) : r2.x),
+                                            rsqrtf(POT ? fmaxf(r2.y, 1e-30f) : r2.y));
             // spline for u = r/h_g < 1 (kernel.h:452-470), Newtonian beyond (:391-398);
             // the two meet at u = 1, where the spline's force factor is 1/u^3
-            const float u = r2 * rinv * hinv, iu = hg * rinv;
-            float wp;
-            const float wf = spline_wf(u, iu, &wp);
-            const bool soft = u < 1.f;
-            float fpot, fac = 0.f;
+            const float2 u = mul2(mul2(r2, rinv), hinv), iu = mul2(hg, rinv);
+            float2 wp;
+            const float2 wf = spline_wf2(u, iu, &wp);
+            const bool sx = u.x < 1.f, sy = u.y < 1.f;
+            float2 fpot, fac = dup2(0.f);
             if (HOMOG) {   // Newtonian as m/h_g^3 (1/u)^3 and -m/h_g (1/u), on the entry's products
-                fpot = hh.z * (soft ? wp : -iu);
-                if (!POT) fac = hh.w * (soft ? wf : iu * iu * iu);
+                fpot = mul2(mh, sel2(sx, sy, wp, make_float2(-iu.x, -iu.y)));
+                if (!POT) fac = mul2(mh3, sel2(sx, sy, wf, mul2(mul2(iu, iu), iu)));
             } else {
-                const float mr = e.w * rinv;
-                fpot = soft ? e.w * wp * hinv : -mr;
-                if (!POT) fac = soft ? e.w * wf * (hinv * hinv * hinv) : mr * rinv * rinv;
+                const float2 mr = mul2(em, rinv);
+                fpot = sel2(sx, sy, mul2(mul2(em, wp), hinv), make_float2(-mr.x, -mr.y));
+                if (!POT)
+                    fac = sel2(sx, sy, mul2(mul2(em, wf), mul2(mul2(hinv, hinv), hinv)), mul2(mul2(mr, rinv), rinv));
             }
             if (POT) {
-                pp[s] += fpot;
+                pp[s] = add2(pp[s], fpot);
             } else {
-                const bool use = r2 > 0.f;
-                fac = use ? fac : 0.f;
-                fpot = use ? fpot : 0.f;
-                self[s] += use ? 0 : 1;
-                px[s] = fmaf(dx, fac, px[s]);
-                py[s] = fmaf(dy, fac, py[s]);
-                pz[s] = fmaf(dz, fac, pz[s]);
-                pp[s] += fpot;
+                const bool ux = r2.x > 0.f, uy = r2.y > 0.f;
+                fac = sel2(ux, uy, fac, dup2(0.f));
+                fpot = sel2(ux, uy, fpot, dup2(0.f));
+                self[s] += (ux ? 0 : 1) + (uy ? 0 : 1);
+                px[s] = fma2(dx, fac, px[s]);
+                py[s] = fma2(dy, fac, py[s]);
+                pz[s] = fma2(dz, fac, pz[s]);
+                pp[s] = add2(pp[s], fpot);
             }
         }
     }
 #pragma unroll
     for (int s = 0; s < TPL; s++) {
-        if (!POT) { T.ax[s].add(px[s]); T.ay[s].add(py[s]); T.az[s].add(pz[s]); }
-        T.pot[s].add(pp[s]);
+        if (!POT) {
+            T.ax[s].add(px[s].x + px[s].y);
+            T.ay[s].add(py[s].x + py[s].y);
+            T.az[s].add(pz[s].x + pz[s].y);
+        }
+        T.pot[s].add(pp[s].x + pp[s].y);
         T.nint[s] += nn - self[s];
     }
     __syncwarp();
 }
 
 template <int TPL, bool POT>
-__device__ __forceinline__ void flush_near_sel(bool homog, const float4 *__restrict__ nearE,
-                                               const float4 *__restrict__ nearH, int nn, Targets<TPL> &T)
+__device__ __forceinline__ void flush_near_sel(bool homog, float *__restrict__ nearE, float *__restrict__ nearH,
+                                               int nn, Targets<TPL> &T)
 {
     if (homog) flush_near<TPL, POT, true>(nearE, nearH, nn, T);
     else flush_near<TPL, POT, false>(nearE, nearH, nn, T);
@@ -297,12 +366,12 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
     extern __shared__ float4 walk_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
-    const int FL = p.flush, cap = FL + 32;
-    float4 *far = walk_smem + (size_t)warp * walk_warp_float4s(FL);
-    float4 *nearE = far + cap;
-    float4 *nearH = nearE + cap;
-    int *sstack = reinterpret_cast<int *>(far + 3 * cap);
-    int4 *nslot = reinterpret_cast<int4 *>(far + 3 * cap + WALK_SSTACK / 4) + 4 * lane;
+    const int FL = p.flush, cap = list_cap(FL);
+    float *far = reinterpret_cast<float *>(walk_smem + (size_t)warp * walk_warp_float4s(FL));
+    float *nearE = far + 4 * cap;
+    float *nearH = nearE + 4 * cap;
+    int *sstack = reinterpret_cast<int *>(far + 12 * cap);
+    int4 *nslot = reinterpret_cast<int4 *>(far + 12 * cap + WALK_SSTACK) + 4 * lane;
     int *gstack = p.stack + (size_t)(blockIdx.x * WALK_WARPS + warp) * p.stack_cap;
     const int ngroups = *p.ngroups;
     const double theta = p.theta;
@@ -481,11 +550,11 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
                 unsigned mf = __ballot_sync(FULL, act == 1 && isfar);
                 unsigned mn = __ballot_sync(FULL, act == 1 && !isfar);
                 if (act == 1) {
-                    if (isfar) far[nf + __popc(mf & lt_mask)] = ent;
+                    if (isfar) list_put(far, nf + __popc(mf & lt_mask), ent);
                     else {
                         int pos = nn + __popc(mn & lt_mask);
-                        nearE[pos] = ent;
-                        nearH[pos] = near_soft(hp, ent.w, homog, hmax);
+                        list_put(nearE, pos, ent);
+                        list_put(nearH, pos, near_soft(hp, ent.w, homog, hmax));
                     }
                 }
                 nf += __popc(mf);
@@ -562,11 +631,11 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
                     unsigned mf = __ballot_sync(FULL, use && pfar);
                     unsigned mn = __ballot_sync(FULL, use && !pfar);
                     if (use) {
-                        if (pfar) far[nf + __popc(mf & lt_mask)] = pe;
+                        if (pfar) list_put(far, nf + __popc(mf & lt_mask), pe);
                         else {
                             int pos = nn + __popc(mn & lt_mask);
-                            nearE[pos] = pe;
-                            nearH[pos] = near_soft(ph, pe.w, homog, hmax);
+                            list_put(nearE, pos, pe);
+                            list_put(nearH, pos, near_soft(ph, pe.w, homog, hmax));
                         }
                     }
                     nf += __popc(mf);
