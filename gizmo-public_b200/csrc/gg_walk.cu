@@ -40,17 +40,19 @@ int gg_walk_threads() { return WALK_THREADS; }
 
 // Per-warp shared memory, in float4 units:
 //   far list float4[cap] | near list float4[cap] | near softening float4[cap] |
-//   node stack int[WALK_SSTACK] | node slots GGNode[32]
+//   node stack int[WALK_SSTACK] | node slots GGNode[32] | particle queue int[PQ_CAP]
 // with cap = list_cap(flush) entries of 4 floats.  The stack spills to the warp's global stack area
 // when it overflows (deep or wide traversals only).
 #define WALK_SSTACK 512
+// particle queue: indices of the particles of opened leaves, evaluated 32 at a time
+#define PQ_CAP 224
 // list capacity in entries: a flush threshold plus one ballot's worth, even
 // (the lists are stored in pairs)
 __host__ __device__ __forceinline__ int list_cap(int flush) { return (flush + 33) & ~1; }
 __host__ __device__ __forceinline__ int walk_warp_float4s(int flush)
 {
     const int cap = list_cap(flush);
-    return 3 * cap + WALK_SSTACK / 4 + 32 * 4;
+    return 3 * cap + WALK_SSTACK / 4 + 32 * 4 + PQ_CAP / 4;
 }
 
 int gg_walk_smem_bytes(int flush, int tpl)
@@ -354,6 +356,22 @@ __device__ __forceinline__ int warp_incl_scan(int v, int lane)
     }
     return v;
 }
+// exclusive prefix sum over the warp of v in [0, 2^BITS), and the total, from
+// one ballot per bit: the ballots are independent, so the latency is that of
+// one vote, not of a chain of shuffles
+template <int BITS>
+__device__ __forceinline__ int warp_excl_bits(int v, unsigned lt_mask, int *total)
+{
+    int ex = 0, tot = 0;
+#pragma unroll
+    for (int b = 0; b < BITS; b++) {
+        const unsigned m = __ballot_sync(FULL, (v >> b) & 1);
+        ex += __popc(m & lt_mask) << b;
+        tot += __popc(m) << b;
+    }
+    *total = tot;
+    return ex;
+}
 
 // MINB: resident blocks per SM the register allocation must allow (1..3): a
 // tuning knob trading registers (spills) against warps in flight.
@@ -372,6 +390,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
     float *nearH = nearE + 4 * cap;
     int *sstack = reinterpret_cast<int *>(far + 12 * cap);
     int4 *nslot = reinterpret_cast<int4 *>(far + 12 * cap + WALK_SSTACK) + 4 * lane;
+    int *pq = reinterpret_cast<int *>(far + 12 * cap + WALK_SSTACK + 32 * 16);
     int *gstack = p.stack + (size_t)(blockIdx.x * WALK_WARPS + warp) * p.stack_cap;
     const int ngroups = *p.ngroups;
     const double theta = p.theta;
@@ -467,6 +486,46 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
             sp -= k;
             __syncwarp();
             return k;
+        };
+        // evaluate the top m (<= 32) particles of the queue, one per lane:
+        // classify them against the group box and append them to the lists
+        int qn = 0;
+        auto take_particles = [&](int m) {
+            bool use = false, pfar = false;
+            float4 pe = make_float4(0.f, 0.f, 0.f, 0.f);
+            float ph = 0.f;
+            if (lane < m) {
+                const GGPart pp = load_part(p.parts + pq[qn - m + lane]);
+                if (pp.m > 0.f) {
+                    const float dx = (float)(pp.x - cg[0]), dy = (float)(pp.y - cg[1]), dz = (float)(pp.z - cg[2]);
+                    const float ex = fmaxf(fabsf(dx) - hwf[0], 0.f), ey = fmaxf(fabsf(dy) - hwf[1], 0.f),
+                                ez = fmaxf(fabsf(dz) - hwf[2], 0.f);
+                    const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+                    const float hh = fmaxf(hmax, pp.h);
+                    pe = make_float4(dx, dy, dz, pp.m);
+                    ph = pp.h;
+                    use = true;
+                    pfar = (r2 >= hh * hh) && (r2 > FAR_MIN_R2);
+                }
+            }
+            qn -= m;
+            const unsigned mf = __ballot_sync(FULL, use && pfar);   // also orders the queue reads before reuse
+            const unsigned mn = __ballot_sync(FULL, use && !pfar);
+            if (use) {
+                if (pfar) list_put(far, nf + __popc(mf & lt_mask), pe);
+                else {
+                    const int pos = nn + __popc(mn & lt_mask);
+                    list_put(nearE, pos, pe);
+                    list_put(nearH, pos, near_soft(ph, pe.w, homog, hmax));
+                }
+            }
+            nf += __popc(mf);
+            nn += __popc(mn);
+            list_far += __popc(mf);
+            list_near += __popc(mn);
+            if (nf >= FL) { flush_far<TPL, POT>(far, nf, T); nf = 0; }
+            if (nn >= FL) { flush_near_sel<TPL, POT>(homog, nearE, nearH, nn, T); nn = 0; }
+            __syncwarp();
         };
         int node = -1;
         int k = pop_nodes(node);
@@ -565,9 +624,9 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
             // opened internal nodes -> children on the stack (spilling its
             // bottom half to global memory when it would overflow)
             {
-                int nch = (act == 2) ? nb : 0;
-                int incl = warp_incl_scan(nch, lane);
-                int total = __shfl_sync(FULL, incl, 31);
+                const int nch = (act == 2) ? nb : 0;   // 1..8 children
+                int total;
+                const int ex = warp_excl_bits<4>(nch, lt_mask, &total);
                 if (sp + total > WALK_SSTACK) {
                     const int m = WALK_SSTACK / 2;
                     if (gsp + m > p.stack_cap) {
@@ -581,7 +640,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
                     gsp += m;
                     sp -= m;
                 }
-                int o = sp + incl - nch;
+                const int o = sp + ex;
                 for (int c = 0; c < nch; c++) sstack[o + c] = na + c;
                 sp += total;
                 __syncwarp();
@@ -593,57 +652,29 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
             if (lane < next_k) stage_node(nslot, p.nodes + next_node);
             if (nf >= FL) { flush_far<TPL, POT>(far, nf, T); nf = 0; }
             if (nn >= FL) { flush_near_sel<TPL, POT>(homog, nearE, nearH, nn, T); nn = 0; }
-            // opened leaves -> particles, 32 at a time
+            // opened leaves -> their particles onto the particle queue, which
+            // is evaluated 32 particles at a time (leftovers wait for later
+            // rounds).  A push that does not fit is taken in parts, the queue
+            // drained between them.
             {
-                int cnt = (act == 3) ? -nb : 0;
-                int incl = warp_incl_scan(cnt, lane);
-                int P = __shfl_sync(FULL, incl, 31);
-                int excl = incl - cnt;
-                for (int pb = 0; pb < P; pb += 32) {
-                    int q = pb + lane;
-                    int src = 0;
-#pragma unroll
-                    for (int step = 16; step > 0; step >>= 1) {
-                        int v = __shfl_sync(FULL, incl, src + step - 1);
-                        if (v <= q) src += step;
+                int first = na, rem = (act == 3) ? -nb : 0;
+                while (__any_sync(FULL, rem > 0)) {
+                    int P, ex;
+                    if (__any_sync(FULL, rem >= 64)) {
+                        const int incl = warp_incl_scan(rem, lane);
+                        P = __shfl_sync(FULL, incl, 31);
+                        ex = incl - rem;
+                    } else {
+                        ex = warp_excl_bits<6>(rem, lt_mask, &P);
                     }
-                    src = min(src, 31);
-                    int a_src = __shfl_sync(FULL, na, src);
-                    int e_src = __shfl_sync(FULL, excl, src);
-                    bool use = false, pfar = false;
-                    float4 pe = make_float4(0.f, 0.f, 0.f, 0.f);
-                    float ph = 0.f;
-                    if (q < P) {
-                        int pi = a_src + (q - e_src);
-                        GGPart pp = load_part(p.parts + pi);
-                        if (pp.m > 0.f) {
-                            const float dx = (float)(pp.x - cg[0]), dy = (float)(pp.y - cg[1]), dz = (float)(pp.z - cg[2]);
-                            const float ex = fmaxf(fabsf(dx) - hwf[0], 0.f), ey = fmaxf(fabsf(dy) - hwf[1], 0.f),
-                                        ez = fmaxf(fabsf(dz) - hwf[2], 0.f);
-                            const float r2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-                            const float hh = fmaxf(hmax, pp.h);
-                            pe = make_float4(dx, dy, dz, pp.m);
-                            ph = pp.h;
-                            use = true;
-                            pfar = (r2 >= hh * hh) && (r2 > FAR_MIN_R2);
-                        }
-                    }
-                    unsigned mf = __ballot_sync(FULL, use && pfar);
-                    unsigned mn = __ballot_sync(FULL, use && !pfar);
-                    if (use) {
-                        if (pfar) list_put(far, nf + __popc(mf & lt_mask), pe);
-                        else {
-                            int pos = nn + __popc(mn & lt_mask);
-                            list_put(nearE, pos, pe);
-                            list_put(nearH, pos, near_soft(ph, pe.w, homog, hmax));
-                        }
-                    }
-                    nf += __popc(mf);
-                    nn += __popc(mn);
-                    list_far += __popc(mf);
-                    list_near += __popc(mn);
-                    if (nf >= FL) { flush_far<TPL, POT>(far, nf, T); nf = 0; }
-                    if (nn >= FL) { flush_near_sel<TPL, POT>(homog, nearE, nearH, nn, T); nn = 0; }
+                    const int room = PQ_CAP - qn;
+                    const int take = min(max(room - ex, 0), rem);
+                    for (int c = 0; c < take; c++) pq[qn + ex + c] = first + c;
+                    qn += min(P, room);
+                    first += take;
+                    rem -= take;
+                    __syncwarp();
+                    while (qn >= 32) take_particles(32);
                 }
             }
             k = next_k;
@@ -653,6 +684,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
             if (lane == 0) atomicOr(p.err, GG_EBIT_STACK_OVERFLOW);
             continue;
         }
+        if (qn > 0) take_particles(qn);
         if (nf > 0) flush_far<TPL, POT>(far, nf, T);
         if (nn > 0) flush_near_sel<TPL, POT>(homog, nearE, nearH, nn, T);
 
