@@ -63,8 +63,8 @@ int gg_walk_smem_bytes(int flush, int tpl)
 
 // The next round's node records are staged in shared memory with cp.async, one
 // 64-byte slot per lane, so no registers are held while the loads are in
-// flight (the walk then fits 3 blocks per SM).  A lane refills its slot only
-// after its test of the node in it is complete.
+// flight.  A lane refills its slot only after its test of the node in it is
+// complete.  (Staging two rounds ahead, in two slots, measured no faster.)
 __device__ __forceinline__ void stage_node(int4 *slot, const GGNode *src)
 {
     const unsigned d = (unsigned)__cvta_generic_to_shared(slot);
@@ -356,20 +356,16 @@ __device__ __forceinline__ int warp_incl_scan(int v, int lane)
     }
     return v;
 }
-// exclusive prefix sum over the warp of v in [0, 2^BITS), and the total, from
-// one ballot per bit: the ballots are independent, so the latency is that of
-// one vote, not of a chain of shuffles
+// exclusive prefix sum over the warp of v in [0, 2^BITS) from one ballot per
+// bit, and the total from one reduction: the votes are independent, so the
+// latency is that of one vote, not of a chain of shuffles
 template <int BITS>
 __device__ __forceinline__ int warp_excl_bits(int v, unsigned lt_mask, int *total)
 {
-    int ex = 0, tot = 0;
+    int ex = 0;
 #pragma unroll
-    for (int b = 0; b < BITS; b++) {
-        const unsigned m = __ballot_sync(FULL, (v >> b) & 1);
-        ex += __popc(m & lt_mask) << b;
-        tot += __popc(m) << b;
-    }
-    *total = tot;
+    for (int b = 0; b < BITS; b++) ex += __popc(__ballot_sync(FULL, (v >> b) & 1) & lt_mask) << b;
+    *total = (int)__reduce_add_sync(FULL, (unsigned)v);
     return ex;
 }
 
@@ -389,7 +385,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
     float *nearE = far + 4 * cap;
     float *nearH = nearE + 4 * cap;
     int *sstack = reinterpret_cast<int *>(far + 12 * cap);
-    int4 *nslot = reinterpret_cast<int4 *>(far + 12 * cap + WALK_SSTACK) + 4 * lane;
+    int4 *const nslot = reinterpret_cast<int4 *>(far + 12 * cap + WALK_SSTACK) + 4 * lane;
     int *pq = reinterpret_cast<int *>(far + 12 * cap + WALK_SSTACK + 32 * 16);
     int *gstack = p.stack + (size_t)(blockIdx.x * WALK_WARPS + warp) * p.stack_cap;
     const int ngroups = *p.ngroups;
@@ -660,12 +656,15 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
                 int first = na, rem = (act == 3) ? -nb : 0;
                 while (__any_sync(FULL, rem > 0)) {
                     int P, ex;
-                    if (__any_sync(FULL, rem >= 64)) {
+                    const unsigned big = __ballot_sync(FULL, rem >= 16);
+                    if (!big) {
+                        ex = warp_excl_bits<4>(rem, lt_mask, &P);   // leaves of up to 15 particles
+                    } else if (!__any_sync(FULL, rem >= 64)) {
+                        ex = warp_excl_bits<6>(rem, lt_mask, &P);
+                    } else {
                         const int incl = warp_incl_scan(rem, lane);
                         P = __shfl_sync(FULL, incl, 31);
                         ex = incl - rem;
-                    } else {
-                        ex = warp_excl_bits<6>(rem, lt_mask, &P);
                     }
                     const int room = PQ_CAP - qn;
                     const int take = min(max(room - ex, 0), rem);
@@ -680,6 +679,7 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
             k = next_k;
             node = next_node;
         }
+        asm volatile("cp.async.wait_all;" ::: "memory");   // no copy into the slot outlives its group
         if (overflow) {
             if (lane == 0) atomicOr(p.err, GG_EBIT_STACK_OVERFLOW);
             continue;
