@@ -283,7 +283,8 @@ def run_ensemble(args, torch, ggb200, dist, world, rank, local):
     tol = args.tol
 
     tree = ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush, device=local,
-                              blocks_per_sm=args.blocks_per_sm, group_order=args.group_order)
+                              blocks_per_sm=args.blocks_per_sm, group_order=args.group_order,
+                              node_staging=args.node_staging)
     tree.set_stream(stream.cuda_stream)
     tree.load_device(d_rec, counts)
     tree.build()
@@ -345,7 +346,8 @@ def run_ensemble(args, torch, ggb200, dist, world, rank, local):
     d_acc_p = torch.empty((n, 3), dtype=torch.float64, device=dev)
     d_pot_p = torch.empty(n, dtype=torch.float64, device=dev)
     plain = ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush, device=local,
-                               blocks_per_sm=args.blocks_per_sm, group_order=args.group_order)
+                               blocks_per_sm=args.blocks_per_sm, group_order=args.group_order,
+                              node_staging=args.node_staging)
     plain.set_stream(stream.cuda_stream)
 
     def plain_pass():
@@ -385,7 +387,8 @@ def run_ensemble(args, torch, ggb200, dist, world, rank, local):
         with ggb200.GravityTree(leaf_size=tuned["leaf_size"] if tuned else args.leaf,
                                 group_size=tuned["group_size"] if tuned else args.group,
                                 flush=tuned["flush"] if tuned else args.flush, device=local,
-                                blocks_per_sm=tuned["blocks_per_sm"] if tuned else args.blocks_per_sm) as te:
+                                blocks_per_sm=tuned["blocks_per_sm"] if tuned else args.blocks_per_sm,
+                                node_staging=tuned["node_staging"] if tuned else args.node_staging) as te:
             old_h = np.linalg.norm(acc_b, axis=1)
 
             def e2e_step():
@@ -572,7 +575,7 @@ def run_split(args, torch, ggb200, dist, world, rank, local):
     d_pot = torch.empty(share[rank], dtype=torch.float64, device=dev)
     tree = ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush, device=local,
                               blocks_per_sm=args.blocks_per_sm, target_order=args.target_order,
-                              group_order=args.group_order)
+                              group_order=args.group_order, node_staging=args.node_staging)
     tree.set_stream(stream.cuda_stream)
     split = multi.SplitSystem(dist, tree, torch, dev)
     split.step(d_rec, d_acc, d_pot, err_tol_theta=0.7)
@@ -674,6 +677,8 @@ def main():
     ap.add_argument("--flush", type=int, default=64)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--target-order", type=int, default=1, choices=[0, 1])
+    ap.add_argument("--node-staging", type=int, default=0, choices=[0, 1],
+                    help="walk node staging: 0 per-lane cp.async, 1 bulk copies (TMA)")
     ap.add_argument("--group-order", type=int, default=1, choices=[0, 1],
                     help="1: walk groups handed out most expensive first, by the previous walk's costs")
     ap.add_argument("--no-autotune", action="store_true")
@@ -720,7 +725,8 @@ def main():
 
     tree = ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush,
                               device=local, blocks_per_sm=args.blocks_per_sm,
-                              target_order=args.target_order, group_order=args.group_order)
+                              target_order=args.target_order, group_order=args.group_order,
+                              node_staging=args.node_staging)
     tree.set_stream(stream.cuda_stream)
     tree.load_device(d_rec, [n])
     # start-up Barnes-Hut pass gives OldAcc (accel.c:47-50), left on the device
@@ -787,7 +793,7 @@ def main():
     # stage breakdown on one extra instrumented step (outside the timed region)
     tprof = ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush, device=local,
                                timing=True, blocks_per_sm=args.blocks_per_sm, target_order=args.target_order,
-                              group_order=args.group_order)
+                              group_order=args.group_order, node_staging=args.node_staging)
     tprof.set_stream(stream.cuda_stream)
     tprof.load_device(d_rec, [n])
     tprof.build()
@@ -849,7 +855,8 @@ def main():
             old = torch.linalg.norm(d_acc, dim=1).cpu().numpy()
         with ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush,
                                 device=local, blocks_per_sm=args.blocks_per_sm,
-                              target_order=args.target_order, group_order=args.group_order) as te:
+                              target_order=args.target_order, group_order=args.group_order,
+                              node_staging=args.node_staging) as te:
             out = (np.empty((na, 3)), np.empty(na))   # the caller's result arrays, reused every step
 
             def e2e_step():
@@ -885,6 +892,7 @@ def main():
                    "l2": "inputs larger than L2 (32 B/particle records, 134 MB + tree)",
                    "leaf_size": args.leaf, "group_size": args.group, "flush": args.flush,
                    "group_order": "by previous walk's cost" if args.group_order else "target order",
+                   "node_staging": ["cp.async per lane", "bulk copies (TMA) per run"][args.node_staging],
                    "parallelism": "independent system per GPU" if world > 1 else "1 GPU"},
         "force_error": {"p50": p50, "p99": p99, "targets": ne, "vs": "FP64 direct sum (GPU, same pair rule)",
                         "pot_sum_rel_diff_sample": abs(wsum - wsum_dir) / abs(wsum_dir)},

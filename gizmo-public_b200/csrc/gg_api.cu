@@ -298,6 +298,7 @@ extern "C" void gg_config_default(gg_config *cfg)
     cfg->timing = 0;
     cfg->target_order = 1;
     cfg->group_order = 1;
+    cfg->node_staging = 0;
 }
 
 extern "C" const char *gg_strerror(gg_status s)
@@ -345,6 +346,7 @@ extern "C" gg_status gg_create(const gg_config *cfg, gg_ctx **out)
     if (c.group_size < 1 || c.group_size > 64) return GG_ERR_INVALID;
     if (c.flush_threshold < 32 || c.flush_threshold > 128) return GG_ERR_INVALID;
     if (c.group_order != 0 && c.group_order != 1) return GG_ERR_INVALID;
+    if (c.node_staging != 0 && c.node_staging != 1) return GG_ERR_INVALID;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= c.device || c.device < 0) {
         cudaGetLastError();
@@ -713,6 +715,7 @@ static gg_status run_walk(gg_ctx *c, const int *d_active, int n_active, const do
     p.pot_only = pot_only ? 1 : 0;
     if (pot_only) p.acc = nullptr;
     p.gorder = gorder;
+    p.node_staging = c->cfg.node_staging;
     p.cost_out = c->cfg.group_order ? c->tcost.p : nullptr;
     int tpl = c->cfg.group_size > 32 ? 2 : 1;
     if (c->cfg.timing) cudaEventRecord(c->ev[4], s);
@@ -966,7 +969,8 @@ extern "C" gg_status gg_graph_launch(gg_ctx *c)
 
 // Timed search over the walk's tunables on the resident systems: leaf size
 // (rebuilds the tree), group size (targets per warp), blocks per SM (stack
-// depth per warp follows from it) and the list-flush threshold.  Every trial
+// depth per warp follows from it) and the list-flush threshold; then the
+// other node staging on the winner.  Every trial
 // walks from the same OldAcc, so trials see the same opening decisions for a
 // given tree; the fastest configuration is kept and the tree rebuilt with it.
 extern "C" gg_status gg_autotune(gg_ctx *c, double tol, double theta, gg_config *chosen, double *best_ms)
@@ -992,6 +996,28 @@ extern "C" gg_status gg_autotune(gg_ctx *c, double tol, double theta, gg_config 
     gg_config best_cfg = base;
     int best_blocks = base_blocks;
     st = GG_OK;
+    // one configuration: the faster of two timed walks from the same OldAcc
+    auto trial = [&](float *ms_out) -> gg_status {
+        float ms_min = 1e30f;
+        for (int rep = 0; rep < 2; rep++) {
+            if (had_old) {
+                cudaError_t ce =
+                    cudaMemcpyAsync(c->oldacc.p, c->oldacc_save.p, N * sizeof(double), cudaMemcpyDeviceToDevice, s);
+                if (ce != cudaSuccess) return gg_cuda_fail(ce);
+            }
+            c->oldacc_valid = had_old;
+            cudaEventRecord(e0, s);
+            gg_status r = run_walk(c, nullptr, 0, nullptr, tol, theta, c->acc_d.p, nullptr, nullptr);
+            cudaEventRecord(e1, s);
+            if (r) return r;
+            if ((r = collect_stats(c, nullptr))) return r;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < ms_min) ms_min = ms;
+        }
+        *ms_out = ms_min;
+        return GG_OK;
+    };
     for (int li = 0; li < 2 && !st; li++) {
         c->cfg.leaf_size = leafs[li];
         if ((st = gg_build(c, nullptr))) break;
@@ -1001,29 +1027,25 @@ extern "C" gg_status gg_autotune(gg_ctx *c, double tol, double theta, gg_config 
                     c->cfg.group_size = groups[gi];
                     c->cfg.flush_threshold = flushes[fi];
                     c->walk_blocks = bpss[bi];
-                    float ms_min = 1e30f;
-                    for (int rep = 0; rep < 2 && !st; rep++) {
-                        if (had_old) {
-                            cudaError_t ce = cudaMemcpyAsync(c->oldacc.p, c->oldacc_save.p, N * sizeof(double),
-                                                             cudaMemcpyDeviceToDevice, s);
-                            if (ce != cudaSuccess) { st = gg_cuda_fail(ce); break; }
-                        }
-                        c->oldacc_valid = had_old;
-                        cudaEventRecord(e0, s);
-                        st = run_walk(c, nullptr, 0, nullptr, tol, theta, c->acc_d.p, nullptr, nullptr);
-                        cudaEventRecord(e1, s);
-                        if (st) break;
-                        st = collect_stats(c, nullptr);
-                        float ms = 0;
-                        cudaEventElapsedTime(&ms, e0, e1);
-                        if (ms < ms_min) ms_min = ms;
-                    }
-                    if (!st && ms_min < best) {
-                        best = ms_min;
+                    float ms = 0;
+                    if ((st = trial(&ms))) break;
+                    if (ms < best) {
+                        best = ms;
                         best_cfg = c->cfg;
                         best_blocks = c->walk_blocks;
                     }
                 }
+    }
+    // the other node staging, on the winner
+    if (!st) {
+        c->cfg = best_cfg;
+        c->walk_blocks = best_blocks;
+        c->cfg.node_staging = 1 - best_cfg.node_staging;
+        float ms = 0;
+        if (!(st = gg_build(c, nullptr)) && !(st = trial(&ms)) && ms < best) {
+            best = ms;
+            best_cfg = c->cfg;
+        }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -55,6 +55,7 @@ struct WalkParams {
     int pot_only;               // potential-only walk: acc and oldacc_out unused, pot required
     const unsigned *gorder;     // order in which groups are handed out, NULL = index order
     float *cost_out;            // per particle (load order): its group's cycles per target, may be NULL
+    int node_staging;           // 0: per-lane cp.async, 1: bulk copies (TMA) per run of consecutive nodes
 };
 int gg_walk_smem_bytes(int flush, int tpl);
 void gg_launch_walk(const WalkParams &p, int tpl, int blocks_per_sm, cudaStream_t st);

@@ -40,7 +40,8 @@ int gg_walk_threads() { return WALK_THREADS; }
 
 // Per-warp shared memory, in float4 units:
 //   far list float4[cap] | near list float4[cap] | near softening float4[cap] |
-//   node stack int[WALK_SSTACK] | node slots GGNode[32] | particle queue int[PQ_CAP]
+//   node stack int[WALK_SSTACK] | node slots GGNode[32] | particle queue int[PQ_CAP] |
+//   mbarrier of the node copies (16 bytes)
 // with cap = list_cap(flush) entries of 4 floats.  The stack spills to the warp's global stack area
 // when it overflows (deep or wide traversals only).
 #define WALK_SSTACK 512
@@ -52,7 +53,7 @@ __host__ __device__ __forceinline__ int list_cap(int flush) { return (flush + 33
 __host__ __device__ __forceinline__ int walk_warp_float4s(int flush)
 {
     const int cap = list_cap(flush);
-    return 3 * cap + WALK_SSTACK / 4 + 32 * 4 + PQ_CAP / 4;
+    return 3 * cap + WALK_SSTACK / 4 + 32 * 4 + PQ_CAP / 4 + 1;
 }
 
 int gg_walk_smem_bytes(int flush, int tpl)
@@ -61,10 +62,16 @@ int gg_walk_smem_bytes(int flush, int tpl)
     return WALK_WARPS * walk_warp_float4s(flush) * 16;
 }
 
-// The next round's node records are staged in shared memory with cp.async, one
-// 64-byte slot per lane, so no registers are held while the loads are in
-// flight.  A lane refills its slot only after its test of the node in it is
-// complete.  (Staging two rounds ahead, in two slots, measured no faster.)
+// ---- staging of node records
+// The next round's node records are copied into shared memory, one 64-byte slot
+// per lane, while this round's leaves and flushes are processed; no registers
+// are held while the copies are in flight.  A lane's slot is refilled only
+// after its test of the node in it is complete.  Two ways (gg_config
+// .node_staging), measured close to each other:
+//  0: each lane copies its own record with cp.async (16-byte pieces through
+//     L1, where the top levels of the tree, which every group visits, hit);
+//  1: the bulk-copy (TMA) engine, one copy per run of consecutive records.
+// (Staging two rounds ahead, in two slots, measured no faster.)
 __device__ __forceinline__ void stage_node(int4 *slot, const GGNode *src)
 {
     const unsigned d = (unsigned)__cvta_generic_to_shared(slot);
@@ -74,14 +81,51 @@ __device__ __forceinline__ void stage_node(int4 *slot, const GGNode *src)
         asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d + 16 * i), "l"(s + i) : "memory");
     asm volatile("cp.async.commit_group;" ::: "memory");
 }
-__device__ __forceinline__ GGNode staged_node(const int4 *slot)
+
+// Bulk copies: the nodes a round pops sit in
+// consecutive lanes, and the children of one node are consecutive records, so
+// they form a few runs of consecutive records: the first lane of each run
+// issues one cp.async.bulk for the whole run.  The copies complete on the
+// warp's mbarrier, which lane 0 arms with the round's byte count; the test
+// waits on the barrier's phase.  Every wait is bounded: after WALK_WAIT_LIMIT
+// polls the warp records GG_EBIT_WALK_TIMEOUT, waits once more (bounded) for
+// its copies and leaves the kernel.
+#define WALK_WAIT_LIMIT (1 << 20)
+
+__device__ __forceinline__ void stage_nodes(unsigned bar, unsigned slot0, const GGNode *nodes, int node, int k,
+                                            int lane)
 {
-    asm volatile("cp.async.wait_all;" ::: "memory");
-    GGNode r;
-    int4 *d = reinterpret_cast<int4 *>(&r);
-#pragma unroll
-    for (int i = 0; i < 4; i++) d[i] = slot[i];
-    return r;
+    const int prev = __shfl_up_sync(FULL, node, 1);
+    const bool start = lane < k && (lane == 0 || node != prev + 1);
+    const unsigned starts = __ballot_sync(FULL, start);
+    // the slots were read by this round's tests, whose values were consumed
+    // before the pop above (warp-synchronous): the copies may overwrite them
+    if (lane == 0)
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(k * 64) : "memory");
+    __syncwarp();
+    if (start) {
+        const unsigned later = starts & ~((2u << lane) - 1u);   // run starts after this lane
+        const int end = later ? __ffs(later) - 1 : k;
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                     ::"r"(slot0 + 64u * lane), "l"(nodes + node), "r"(64u * (end - lane)), "r"(bar)
+                     : "memory");
+    }
+}
+
+// true once the phase of the given parity has completed; false if the bounded
+// wait gave up
+__device__ __forceinline__ bool bar_wait(unsigned bar, unsigned parity)
+{
+    for (int i = 0; i < WALK_WAIT_LIMIT; i++) {
+        unsigned done;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(bar), "r"(parity)
+                     : "memory");
+        if (done) return true;
+    }
+    return false;
 }
 
 __device__ __forceinline__ GGPart load_part(const GGPart *p)
@@ -374,7 +418,7 @@ __device__ __forceinline__ int warp_excl_bits(int v, unsigned lt_mask, int *tota
 // F64T: opening tests in FP64 (used for one-target groups, where the tests are
 // exactly the reference's); otherwise the tests run in FP32 on FP64-formed
 // offsets from the group centre, against a bounding box rounded outwards.
-template <int TPL, int MINB, bool F64T, bool POT>
+template <int TPL, int MINB, bool F64T, bool POT, bool TMA = false>
 __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
 {
     extern __shared__ float4 walk_smem[];
@@ -386,7 +430,16 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
     float *nearH = nearE + 4 * cap;
     int *sstack = reinterpret_cast<int *>(far + 12 * cap);
     int4 *const nslot = reinterpret_cast<int4 *>(far + 12 * cap + WALK_SSTACK) + 4 * lane;
+    const unsigned slot0 = (unsigned)__cvta_generic_to_shared(far + 12 * cap + WALK_SSTACK);
     int *pq = reinterpret_cast<int *>(far + 12 * cap + WALK_SSTACK + 32 * 16);
+    const unsigned bar = (unsigned)__cvta_generic_to_shared(far + 12 * cap + WALK_SSTACK + 32 * 16 + PQ_CAP);
+    if (lane == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    unsigned phase = 0;   // parity of the barrier phase the next wait is for
+    constexpr bool tma = TMA;   // node staging by bulk copies (else per-lane cp.async)
     int *gstack = p.stack + (size_t)(blockIdx.x * WALK_WARPS + warp) * p.stack_cap;
     const int ngroups = *p.ngroups;
     const double theta = p.theta;
@@ -525,16 +578,32 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
         };
         int node = -1;
         int k = pop_nodes(node);
-        if (lane < k) stage_node(nslot, p.nodes + node);
+        if (tma) {
+            if (k > 0) stage_nodes(bar, slot0, p.nodes, node, k, lane);   // one barrier phase per staged round
+        } else if (lane < k) {
+            stage_node(nslot, p.nodes + node);
+        }
+        bool timed_out = false;
         while (k > 0) {
             tested += k;
+            if (tma) {
+                if (!bar_wait(bar, phase)) {
+                    timed_out = true;
+                    break;
+                }
+                phase ^= 1u;
+            } else {
+                asm volatile("cp.async.wait_all;" ::: "memory");
+            }
 
             int act = 0, na = 0, nb = 0;
             bool isfar = false;
             float4 ent = make_float4(0.f, 0.f, 0.f, 0.f);
             float hp = 0.f;
             if (lane < k) {
-                const GGNode nd = staged_node(nslot);
+                GGNode nd;
+#pragma unroll
+                for (int i = 0; i < 4; i++) reinterpret_cast<int4 *>(&nd)[i] = nslot[i];
                 na = nd.a;
                 nb = nd.b;
                 if (nd.mass > 0.f) {
@@ -645,7 +714,11 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
             // this round's flushes and leaf particles
             int next_node = -1;
             const int next_k = pop_nodes(next_node);
-            if (lane < next_k) stage_node(nslot, p.nodes + next_node);
+            if (tma) {
+                if (next_k > 0) stage_nodes(bar, slot0, p.nodes, next_node, next_k, lane);
+            } else if (lane < next_k) {
+                stage_node(nslot, p.nodes + next_node);
+            }
             if (nf >= FL) { flush_far<TPL, POT>(far, nf, T); nf = 0; }
             if (nn >= FL) { flush_near_sel<TPL, POT>(homog, nearE, nearH, nn, T); nn = 0; }
             // opened leaves -> their particles onto the particle queue, which
@@ -679,7 +752,12 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
             k = next_k;
             node = next_node;
         }
-        asm volatile("cp.async.wait_all;" ::: "memory");   // no copy into the slot outlives its group
+        if (!tma) asm volatile("cp.async.wait_all;" ::: "memory");   // no copy into the slot outlives its group
+        if (timed_out) {   // copies may still be in flight: wait once more, then leave
+            if (lane == 0) atomicOr(p.err, GG_EBIT_WALK_TIMEOUT);
+            bar_wait(bar, phase);
+            return;
+        }
         if (overflow) {
             if (lane == 0) atomicOr(p.err, GG_EBIT_STACK_OVERFLOW);
             continue;
@@ -727,11 +805,11 @@ __global__ void __launch_bounds__(WALK_THREADS, MINB) k_walk(WalkParams p)
     }
 }
 
-template <int TPL, int MINB, bool F64T, bool POT = false>
+template <int TPL, int MINB, bool F64T, bool POT = false, bool TMA = false>
 static void launch_walk_t(const WalkParams &p, int blocks, int smem, cudaStream_t st)
 {
-    cudaFuncSetAttribute(k_walk<TPL, MINB, F64T, POT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    k_walk<TPL, MINB, F64T, POT><<<blocks, WALK_THREADS, smem, st>>>(p);
+    cudaFuncSetAttribute(k_walk<TPL, MINB, F64T, POT, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k_walk<TPL, MINB, F64T, POT, TMA><<<blocks, WALK_THREADS, smem, st>>>(p);
 }
 
 // blocks_per_sm selects the register budget of the instantiation (1..3) and
@@ -747,6 +825,14 @@ void gg_launch_walk(const WalkParams &p, int tpl, int blocks_per_sm, cudaStream_
         else launch_walk_t<1, 2, false, true>(p, blocks, smem, st);
     } else if (p.group_size == 1) {
         launch_walk_t<1, 2, true>(p, blocks, smem, st);   // exact mode: the reference's tests
+    } else if (p.node_staging == 1) {   // bulk-copy node staging (the force walk's tuned forms)
+        if (tpl == 2) {
+            if (minb == 3) launch_walk_t<2, 3, false, false, true>(p, blocks, smem, st);
+            else launch_walk_t<2, 2, false, false, true>(p, blocks, smem, st);
+        } else {
+            if (minb == 3) launch_walk_t<1, 3, false, false, true>(p, blocks, smem, st);
+            else launch_walk_t<1, 2, false, false, true>(p, blocks, smem, st);
+        }
     } else if (tpl == 2) {
         if (minb == 1) launch_walk_t<2, 1, false>(p, blocks, smem, st);
         else if (minb == 2) launch_walk_t<2, 2, false>(p, blocks, smem, st);

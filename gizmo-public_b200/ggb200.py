@@ -49,7 +49,8 @@ class GravityError(RuntimeError):
 class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("leaf_size", ctypes.c_int32), ("group_size", ctypes.c_int32),
                 ("flush_threshold", ctypes.c_int32), ("walk_blocks_per_sm", ctypes.c_int32),
-                ("timing", ctypes.c_int32), ("target_order", ctypes.c_int32), ("group_order", ctypes.c_int32)]
+                ("timing", ctypes.c_int32), ("target_order", ctypes.c_int32), ("group_order", ctypes.c_int32),
+                ("node_staging", ctypes.c_int32)]
 
 
 class Domain(ctypes.Structure):
@@ -173,7 +174,7 @@ class GravityTree:
     """One library context: particles of one or more systems, their trees, walks."""
 
     def __init__(self, leaf_size=8, group_size=32, flush=64, device=0, timing=False, blocks_per_sm=0, target_order=1,
-                 group_order=1):
+                 group_order=1, node_staging=0):
         lib = load_library()
         cfg = Config()
         lib.gg_config_default(ctypes.byref(cfg))
@@ -182,6 +183,7 @@ class GravityTree:
         cfg.walk_blocks_per_sm = blocks_per_sm
         cfg.target_order = target_order
         cfg.group_order = group_order
+        cfg.node_staging = node_staging
         h = ctypes.c_void_p()
         _check(lib.gg_create(ctypes.byref(cfg), ctypes.byref(h)), "gg_create")
         self._lib, self._h = lib, h
@@ -389,14 +391,14 @@ class GravityTree:
         _check(self._lib.gg_graph_launch(self._h), "gg_graph_launch")
 
     def autotune(self, err_tol_force_acc=0.0025, err_tol_theta=0.0):
-        """Pick leaf size, group size, blocks per SM and flush threshold by
-        timing the walk of the resident systems; returns (config dict, ms)."""
+        """Pick leaf size, group size, blocks per SM, flush threshold and node
+        staging by timing the walk of the resident systems; returns (config dict, ms)."""
         cfg = Config()
         ms = ctypes.c_double()
         _check(self._lib.gg_autotune(self._h, err_tol_force_acc, err_tol_theta, ctypes.byref(cfg), ctypes.byref(ms)),
                "gg_autotune")
         return dict(leaf_size=cfg.leaf_size, group_size=cfg.group_size, flush=cfg.flush_threshold,
-                    blocks_per_sm=cfg.walk_blocks_per_sm), ms.value
+                    blocks_per_sm=cfg.walk_blocks_per_sm, node_staging=cfg.node_staging), ms.value
 
 
 def gravity_tree(pos, mass, h, G=1.0, err_tol_force_acc=0.0025, err_tol_theta=0.7, active=None, tree=None,

@@ -64,6 +64,12 @@ typedef struct gg_config {
                                  the cost each target had in the previous walk of this context
                                  (its group's device cycles per target); 0: in target order.
                                  The order changes no result, only when each group runs */
+    int32_t node_staging;     /* how the walk stages node records in shared memory: 0 (default):
+                                 each lane copies its own with cp.async (through L1); 1: the
+                                 bulk-copy (TMA) engine, one copy per run of consecutive records,
+                                 completing on an mbarrier (force walks of groups > 1; the
+                                 exact and potential-only walks stage per lane).  Same results;
+                                 gg_autotune tries both */
 } gg_config;
 
 /* root cube of one system: domain_findExtent (domain.c:2518-2570) */

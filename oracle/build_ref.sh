@@ -15,7 +15,7 @@ CC=/usr/bin/gcc
 # x86-64-v3 (AVX2/FMA): the binary runs on the GPU hosts as well as here
 CFLAGS="-O3 -march=x86-64-v3 -fopenmp -std=gnu99 -w"
 if [ ! -d "$REF" ]; then echo "reference tree not found: $REF" >&2; exit 1; fi
-if [ -x "$OUT/gizmo_ref" ] && [ -x "$OUT/gizmo_ref_pot" ] && [ -x "$OUT/gizmo_b200" ] && [ "$OUT/gizmo_b200" -nt "$HERE/ref_main.c" ] && [ "$OUT/gizmo_b200" -nt "$0" ] && [ "$OUT/gizmo_b200" -nt "$HERE/../gizmo-public_b200/host/gravtree_b200.c" ] && [ "$OUT/gizmo_ref_pot" -nt "$HERE/ref_main.c" ]; then
+if [ -x "$OUT/gizmo_ref" ] && [ -x "$OUT/gizmo_ref_pot" ] && [ -x "$OUT/gizmo_b200" ] && [ "$OUT/gizmo_b200" -nt "$HERE/ref_main.c" ] && [ "$OUT/gizmo_b200" -nt "$0" ] && [ "$OUT/gizmo_b200" -nt "$HERE/../gizmo-public_b200/host/gravtree_b200.c" ] && [ "$OUT/gizmo_b200" -nt "$HERE/../include/gizmo_gravity_b200.h" ] && [ "$OUT/gizmo_ref_pot" -nt "$HERE/ref_main.c" ]; then
   echo "oracle/_ref/gizmo_ref is up to date"; exit 0
 fi
 MIRROR="$(mktemp -d /tmp/gg_ref_src.XXXXXX)"
