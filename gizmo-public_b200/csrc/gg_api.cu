@@ -256,6 +256,12 @@ struct gg_ctx {
     long long async_n = 0;
     int async_flags = 0;
     cudaEvent_t act_ev = nullptr, done_ev = nullptr;
+    // host OldAcc of gg_evaluate crosses the link on its own stream into its
+    // own array, while the build runs; the walk waits for it (old_ready_ev) and
+    // the next upload waits for that walk (old_used_ev)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t old_ready_ev = nullptr, old_used_ev = nullptr;
+    DevBuf<double> oldacc_in;
     cudaEvent_t pipe_ev[kPipeEvents] = {};   // completion of each chunk of a pipelined copy to the host
     gg_stats last;
 
@@ -269,7 +275,7 @@ struct gg_ctx {
         f(oldacc); f(vel); f(kin); f(kin_counter); f(dts); f(oldacc_save); f(tcost); f(gkey); f(gorder);
         f(e_chunks); f(e_first); f(e_part); f(e_out);
         f(groups); f(ngroups); f(gscan); f(toff); f(flag); f(flagscan); f(tlist); f(tout); f(scan_scratch);
-        f(active_d); f(counters); f(inter); f(stack); f(err); f(acc_d); f(pot_d); f(nint_d);
+        f(active_d); f(counters); f(inter); f(stack); f(err); f(acc_d); f(pot_d); f(nint_d); f(oldacc_in);
     }
 };
 
@@ -367,7 +373,10 @@ extern "C" gg_status gg_create(const gg_config *cfg, gg_ctx **out)
     if ((e = cudaEventCreateWithFlags(&ctx->stage_ev, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&ctx->vstage_ev, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&ctx->act_ev, cudaEventDisableTiming)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&ctx->done_ev, cudaEventDisableTiming)) != cudaSuccess) {
+        (e = cudaEventCreateWithFlags(&ctx->done_ev, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->old_ready_ev, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->old_used_ev, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking)) != cudaSuccess) {
         gg_destroy(ctx);
         return gg_cuda_fail(e);
     }
@@ -394,6 +403,7 @@ extern "C" gg_status gg_destroy(gg_ctx *c)
     if (!c) return GG_ERR_INVALID;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     c->for_each_buf(ReleaseBuf());
     c->h_active.give_back(c->act_ev);
     c->h_acc.give_back(c->done_ev);
@@ -412,6 +422,9 @@ extern "C" gg_status gg_destroy(gg_ctx *c)
     if (c->graph) cudaGraphDestroy(c->graph);
     if (c->have_events)
         for (int i = 0; i < 8; i++) cudaEventDestroy(c->ev[i]);
+    if (c->old_ready_ev) cudaEventDestroy(c->old_ready_ev);
+    if (c->old_used_ev) cudaEventDestroy(c->old_used_ev);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return GG_OK;
@@ -806,18 +819,26 @@ extern "C" gg_status gg_evaluate(gg_ctx *c, const int32_t *active, int64_t n_act
         }
         d_active = c->active_d.p;
     }
-    if (old_acc) {
-        if ((st = c->h_old.ensure((size_t)c->N, c->done_ev))) return st;
+    const double *d_old = nullptr;
+    if (old_acc && c->N) {
+        // the upload overlaps the build already queued on the compute stream
+        const bool fresh = c->oldacc_in.cap < (size_t)c->N;
+        if ((st = c->h_old.ensure((size_t)c->N, c->done_ev)) || (st = c->oldacc_in.ensure(c->N))) return st;
+        if (fresh) GG_CUDA_TRY(cudaEventRecord(c->old_used_ev, s));   // the new array exists from here on
+        GG_CUDA_TRY(cudaStreamWaitEvent(c->copy_stream, c->old_used_ev, 0));
         for (long long b = 0; b < c->N; b += kPipeChunk) {
             const long long e = std::min((long long)c->N, b + kPipeChunk);
             parallel_copy(c->h_old.p + b, old_acc + b, (size_t)(e - b) * sizeof(double));
-            GG_CUDA_TRY(cudaMemcpyAsync(c->oldacc.p + b, c->h_old.p + b, (e - b) * sizeof(double),
-                                        cudaMemcpyHostToDevice, s));
+            GG_CUDA_TRY(cudaMemcpyAsync(c->oldacc_in.p + b, c->h_old.p + b, (e - b) * sizeof(double),
+                                        cudaMemcpyHostToDevice, c->copy_stream));
         }
-        c->oldacc_valid = true;
+        GG_CUDA_TRY(cudaEventRecord(c->old_ready_ev, c->copy_stream));
+        GG_CUDA_TRY(cudaStreamWaitEvent(s, c->old_ready_ev, 0));
+        d_old = c->oldacc_in.p;
     }
-    if ((st = run_walk(c, d_active, (int)n_active, nullptr, tol, theta, c->acc_d.p, c->pot_d.p, c->nint_d.p)))
+    if ((st = run_walk(c, d_active, (int)n_active, d_old, tol, theta, c->acc_d.p, c->pot_d.p, c->nint_d.p)))
         return st;
+    if (d_old) GG_CUDA_TRY(cudaEventRecord(c->old_used_ev, s));
     // results come back in chunks; each chunk is copied out while the next crosses the link
     long long chunk = kPipeChunk, nchunks = 0;
     if (nt) {
