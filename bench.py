@@ -674,7 +674,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--leaf", type=int, default=8)
     ap.add_argument("--group", type=int, default=32)
-    ap.add_argument("--flush", type=int, default=64)
+    ap.add_argument("--flush", type=int, default=128)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--target-order", type=int, default=1, choices=[0, 1])
     ap.add_argument("--node-staging", type=int, default=0, choices=[0, 1],

@@ -299,7 +299,7 @@ extern "C" void gg_config_default(gg_config *cfg)
     cfg->device = 0;
     cfg->leaf_size = 8;
     cfg->group_size = 32;
-    cfg->flush_threshold = 64;
+    cfg->flush_threshold = 128;
     cfg->walk_blocks_per_sm = 0;
     cfg->timing = 0;
     cfg->target_order = 1;
@@ -1012,7 +1012,7 @@ extern "C" gg_status gg_autotune(gg_ctx *c, double tol, double theta, gg_config 
     GG_CUDA_TRY(cudaEventCreate(&e1));
     const gg_config base = c->cfg;
     const int base_blocks = c->walk_blocks;
-    static const int leafs[] = {8, 16}, groups[] = {32, 64}, bpss[] = {2, 3}, flushes[] = {64, 96};
+    static const int leafs[] = {8, 16}, groups[] = {32, 64}, bpss[] = {2, 3}, flushes[] = {64, 128};
     float best = 1e30f;
     gg_config best_cfg = base;
     int best_blocks = base_blocks;

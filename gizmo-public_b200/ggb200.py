@@ -173,7 +173,7 @@ def domain_to_dict(d):
 class GravityTree:
     """One library context: particles of one or more systems, their trees, walks."""
 
-    def __init__(self, leaf_size=8, group_size=32, flush=64, device=0, timing=False, blocks_per_sm=0, target_order=1,
+    def __init__(self, leaf_size=8, group_size=32, flush=128, device=0, timing=False, blocks_per_sm=0, target_order=1,
                  group_order=1, node_staging=0):
         lib = load_library()
         cfg = Config()

@@ -53,7 +53,7 @@ typedef struct gg_config {
     int32_t device;           /* CUDA device ordinal */
     int32_t leaf_size;        /* max particles per leaf bucket, 1..32 (default 8) */
     int32_t group_size;       /* targets per walk group, 1..64 (default 32) */
-    int32_t flush_threshold;  /* interaction-list entries per flush, 32..128 (default 64) */
+    int32_t flush_threshold;  /* interaction-list entries per flush, 32..128 (default 128) */
     int32_t walk_blocks_per_sm; /* persistent walk blocks per SM, 0 = default */
     int32_t timing;           /* 1: record per-stage device times into gg_stats */
     int32_t target_order;     /* 1 (default): when a system holds several kernel radii, walk
