@@ -4,6 +4,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <omp.h>
 #include <atomic>
 #include <iterator>
 #include <map>
@@ -159,10 +160,13 @@ struct HostBuf {
 };
 
 // host copy spread over the OpenMP threads (results of large batches run to
-// hundreds of MB)
+// hundreds of MB): pieces of at least 256 KB, about four per thread, so that
+// a pipelined chunk of a few MB keeps every thread busy and the copy keeps
+// pace with the link
 static void parallel_copy(void *dst, const void *src, size_t bytes)
 {
-    const size_t chunk = (size_t)4 << 20;
+    const size_t per = bytes / (4 * (size_t)std::max(1, omp_get_max_threads()));
+    const size_t chunk = std::max((size_t)256 << 10, (per + 4095) & ~(size_t)4095);
     const long long nchunks = (long long)((bytes + chunk - 1) / chunk);
     if (nchunks <= 1) { memcpy(dst, src, bytes); return; }
 #pragma omp parallel for schedule(dynamic, 1)
@@ -173,8 +177,9 @@ static void parallel_copy(void *dst, const void *src, size_t bytes)
 }
 
 // Host transfers of large arrays are cut into chunks of this many particles:
-// the host gathers or copies one chunk while the previous one crosses the link.
-static const long long kPipeChunk = 1ll << 20;
+// the host gathers or copies one chunk while the previous one crosses the link
+// (small chunks keep the pipeline's fill and drain short).
+static const long long kPipeChunk = 1ll << 18;
 static const int kPipeEvents = 64;
 
 struct gg_ctx {
