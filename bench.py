@@ -34,10 +34,10 @@ import multi  # noqa: E402
 
 FLOPS_PER_INTERACTION = 20   # monopole force convention (3 sub, r^2, rsqrt, m/r^3, 3 fma)
 # DRAM bytes (read + write) per particle of one k_walk launch on the galaxy,
-# from the ncu capture of the 1,000,000-particle galaxy (111.1 MB read + 36.0 MB
+# from the ncu capture of the 1,000,000-particle galaxy (114.8 MB read + 39.6 MB
 # written); the walk's traffic grows with the particle count, so a launch of
 # the 4.2M galaxy is scaled from it
-WALK_DRAM_BYTES_PER_PARTICLE = {"galaxy": 147.1, "galaxy1m": 147.1}
+WALK_DRAM_BYTES_PER_PARTICLE = {"galaxy": 154.4, "galaxy1m": 154.4}
 METRIC = "tree-gravity particles/s at p99 force err<=2e-3 vs FP64 direct; serve p50/p99 ms"
 
 WORKLOADS = {
