@@ -29,6 +29,18 @@
 // per-target totals with Kahan compensation.  Interactions are counted like
 // the reference (forcetree.c:2258, :2488): one per used node or particle with
 // r^2 > 0 and m > 0.
+//
+// How the work is arranged on the SM (each part is described where it is):
+//   - the next round's node records are staged in shared memory while this
+//     round's leaves and flushes run (per-lane cp.async, or bulk copies of
+//     runs of consecutive records on an mbarrier);
+//   - stack pushes use prefix counts from bit ballots; the particles of opened
+//     leaves go through a per-warp queue and are classified 32 at a time;
+//   - the lists are pair-interleaved and evaluated two entries per packed
+//     FP32x2 instruction;
+//   - the persistent warps take groups in the order the host side planned
+//     (most expensive first, from the previous walk's measured cost), and each
+//     group records its own cost for the next walk.
 #include "gg_internal.cuh"
 #include "gg_kernels.cuh"
 
