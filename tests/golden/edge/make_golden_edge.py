@@ -1,0 +1,61 @@
+#!/usr/bin/env python3
+"""Golden vectors for degenerate inputs, produced by the reference code itself.
+
+Runs oracle/_ref/gizmo_ref (GIZMO's own sources, one OpenMP thread so that its
+interaction counter is exact) on two seeded 600-particle Plummer spheres:
+
+  duplicates_630: 30 particles repeated at exactly the same position (and
+      mass and softening).  Coincident pairs have r = 0: they exert no force
+      on each other and are not counted (forcetree.c:2258).
+  massless_600: 20 particles with zero mass.  GIZMO removes zero-mass
+      particles in rearrange_particle_sequence (merge_split.c:1180-1188),
+      called before every tree build (domain.c:118), so the reference walks
+      and reports only the 580 massive ones; the file keeps which.
+
+Stores the inputs, the reference's Barnes-Hut and relative passes (GravAccel,
+Potential with G = 1, interaction counts) and, for the massless case, the
+mask of the particles the reference kept.  Requires the reference source
+tree, so it runs only where that tree exists; the .npz files it writes are
+committed.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(HERE)))
+sys.path[:0] = [os.path.join(ROOT, "oracle"), os.path.join(ROOT, "gizmo-public_b200")]
+
+import ics  # noqa: E402
+import ref_runner  # noqa: E402
+
+TOL = 0.0025
+
+
+def cases():
+    ic = ics.plummer(600, seed=211)
+    rng = np.random.default_rng(212)
+    dup = rng.choice(600, 30, replace=False)
+    yield "duplicates_630", {k: np.concatenate([ic[k], ic[k][dup]]) for k in ("pos", "vel", "mass", "h")}
+    zero = rng.choice(600, 20, replace=False)
+    m = ic["mass"].copy()
+    m[zero] = 0.0
+    yield "massless_600", dict(pos=ic["pos"], vel=ic["vel"], mass=m, h=ic["h"])
+
+
+def main():
+    for name, ic in cases():
+        r = ref_runner.run(ic, tol=TOL, threads=1)
+        s = r["info"]["startup"]
+        kept = ic["mass"] > 0
+        assert int(s["n"]) == int(kept.sum())
+        np.savez_compressed(
+            os.path.join(HERE, name + ".npz"), pos=ic["pos"], mass=ic["mass"], h=ic["h"], tol=TOL, kept=kept,
+            acc_bh=r["acc_bh"][kept], pot_bh=r["pot_bh"][kept], acc=r["acc"][kept], pot=r["pot"][kept],
+            cost_bh=s["cost_bh"], cost_rel=s["cost_rel"])
+        print(name, "n=%d kept=%d cost_bh=%d cost_rel=%d" % (kept.size, kept.sum(), s["cost_bh"], s["cost_rel"]))
+
+
+if __name__ == "__main__":
+    main()
