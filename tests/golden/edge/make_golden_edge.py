@@ -11,6 +11,11 @@ interaction counter is exact) on two seeded 600-particle Plummer spheres:
       particles in rearrange_particle_sequence (merge_split.c:1180-1188),
       called before every tree build (domain.c:118), so the reference walks
       and reports only the 580 massive ones; the file keeps which.
+  sheet_600: every particle at z = 0 (a flat root cube content).
+  two_2: two particles.
+  lattice_512: an 8x8x8 lattice, so keys tie at every level down to the
+      lattice spacing.
+(A one-particle system stops the reference itself: MPI_Abort(11).)
 
 Stores the inputs, the reference's Barnes-Hut and relative passes (GravAccel,
 Potential with G = 1, interaction counts) and, for the massless case, the
@@ -42,6 +47,16 @@ def cases():
     m = ic["mass"].copy()
     m[zero] = 0.0
     yield "massless_600", dict(pos=ic["pos"], vel=ic["vel"], mass=m, h=ic["h"])
+    ic2 = ics.plummer(600, seed=221)
+    flat = ic2["pos"].copy()
+    flat[:, 2] = 0.0
+    yield "sheet_600", dict(pos=flat, vel=np.zeros_like(flat), mass=ic2["mass"], h=ic2["h"])
+    yield "two_2", dict(pos=ic2["pos"][:2].copy(), vel=np.zeros((2, 3)), mass=ic2["mass"][:2] * 300,
+                        h=ic2["h"][:2].copy())
+    g = np.arange(8, dtype=float)
+    lat = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3) * 0.25
+    n = lat.shape[0]
+    yield "lattice_512", dict(pos=lat, vel=np.zeros_like(lat), mass=np.full(n, 1.0 / n), h=np.full(n, 0.028))
 
 
 def main():

@@ -1,9 +1,10 @@
 """Degenerate inputs pinned to the reference code itself
 (tests/golden/edge/make_golden_edge.py).
 
-Exact duplicates: coincident particles exert no force on each other and are
-not counted, so the oracle reproduces the reference's interaction counts
-exactly and its forces to FP64 rounding.  Massless particles: GIZMO removes
+Exact duplicates, a flat sheet, two particles and a lattice whose keys tie
+down to its spacing: the oracle reproduces the reference's interaction counts
+exactly and its forces and potentials to FP64 rounding (coincident particles
+exert no force on each other and are not counted).  Massless particles: GIZMO removes
 them before every tree build (merge_split.c:1180-1188), so its outputs cover
 the massive particles only; the oracle reproduces them on that subset, and,
 with the massless particles left in, ignores them as sources (the massive
@@ -37,7 +38,16 @@ def close(a, b):
 
 def test_fixtures_present():
     assert sorted(os.path.basename(p) for p in glob.glob(os.path.join(HERE, "*.npz"))) == [
-        "duplicates_630.npz", "massless_600.npz"]
+        "duplicates_630.npz", "lattice_512.npz", "massless_600.npz", "sheet_600.npz", "two_2.npz"]
+
+
+@pytest.mark.parametrize("name", ["sheet_600", "two_2", "lattice_512"])
+def test_degenerate_shapes_match_reference(name):
+    g = load(name)
+    assert g["kept"].all()
+    a1, p1, c1, a2, p2, c2 = two_pass(g["pos"], g["mass"], g["h"], float(g["tol"]))
+    assert c1 == int(g["cost_bh"]) and c2 == int(g["cost_rel"])
+    assert close(a1, g["acc_bh"]) and close(a2, g["acc"]) and close(p2, g["pot"])
 
 
 def test_exact_duplicates_match_reference():
