@@ -18,8 +18,9 @@ interaction counter is exact) on two seeded 600-particle Plummer spheres:
 (A one-particle system stops the reference itself: MPI_Abort(11).)
 
 Stores the inputs, the reference's Barnes-Hut and relative passes (GravAccel,
-Potential with G = 1, interaction counts) and, for the massless case, the
-mask of the particles the reference kept.  Requires the reference source
+Potential with G = 1, interaction counts), the potential-only walk
+(compute_potential, from the build variant without EVALPOTENTIAL) with the
+OldAcc it used, and the mask of the particles the reference kept.  Requires the reference source
 tree, so it runs only where that tree exists; the .npz files it writes are
 committed.
 """
@@ -62,13 +63,15 @@ def cases():
 def main():
     for name, ic in cases():
         r = ref_runner.run(ic, tol=TOL, threads=1)
+        rp = ref_runner.run(ic, tol=TOL, threads=1, binary=ref_runner.BIN_POT)   # compute_potential
         s = r["info"]["startup"]
         kept = ic["mass"] > 0
         assert int(s["n"]) == int(kept.sum())
         np.savez_compressed(
             os.path.join(HERE, name + ".npz"), pos=ic["pos"], mass=ic["mass"], h=ic["h"], tol=TOL, kept=kept,
             acc_bh=r["acc_bh"][kept], pot_bh=r["pot_bh"][kept], acc=r["acc"][kept], pot=r["pot"][kept],
-            cost_bh=s["cost_bh"], cost_rel=s["cost_rel"])
+            cost_bh=s["cost_bh"], cost_rel=s["cost_rel"], pot_only=rp["pot_only"][kept],
+            oldacc_pot=rp["oldacc"][kept])
         print(name, "n=%d kept=%d cost_bh=%d cost_rel=%d" % (kept.size, kept.sum(), s["cost_bh"], s["cost_rel"]))
 
 

@@ -80,3 +80,12 @@ def test_massless_particles_are_ignored_as_sources(tol):
     assert np.isfinite(a2[~k]).all() and (np.linalg.norm(a2[~k], axis=1) > 0).all()
     # only the massless targets' own walks add to the count
     assert c2 > int(g["cost_rel"])
+
+
+@pytest.mark.parametrize("name", ["duplicates_630", "sheet_600", "two_2", "lattice_512", "massless_600"])
+def test_potential_walk_matches_reference(name):
+    g = load(name)
+    k = g["kept"]
+    p = oracle.potential(g["pos"][k], g["mass"][k], g["h"][k], old_acc=g["oldacc_pot"],
+                         err_tol_force_acc=float(g["tol"]))
+    assert np.allclose(p, g["pot_only"], rtol=1e-12, atol=1e-14 * np.abs(g["pot_only"]).max())
