@@ -16,6 +16,10 @@ interaction counter is exact) on two seeded 600-particle Plummer spheres:
   lattice_512: an 8x8x8 lattice, so keys tie at every level down to the
       lattice spacing.
 (A one-particle system stops the reference itself: MPI_Abort(11).)
+  active_10pct_2000: a clustered system of 2,000 particles in which a
+      seeded 10% are active: both start-up passes walk only those (the
+      harness's sample-only mode sets GIZMO's active list), with the tree
+      built from all particles.
 
 Stores the inputs, the reference's Barnes-Hut and relative passes (GravAccel,
 Potential with G = 1, interaction counts), the potential-only walk
@@ -75,5 +79,18 @@ def main():
         print(name, "n=%d kept=%d cost_bh=%d cost_rel=%d" % (kept.size, kept.sum(), s["cost_bh"], s["cost_rel"]))
 
 
+def active_case():
+    ic = ics.clustered(2000, seed=231, n_clumps=10)
+    act = ics.random_active(2000, 0.1, seed=232)
+    r = ref_runner.run(ic, tol=TOL, threads=1, sample=act, sample_only=True)
+    s = r["info"]["startup"]
+    np.savez_compressed(
+        os.path.join(HERE, "active_10pct_2000.npz"), pos=ic["pos"], mass=ic["mass"], h=ic["h"], tol=TOL,
+        active=act, acc_bh=r["acc_bh"][act], acc=r["acc"][act], pot=r["pot"][act], cost_bh=s["cost_bh"],
+        cost_rel=s["cost_rel"])
+    print("active_10pct_2000 active=%d cost_bh=%d cost_rel=%d" % (act.size, s["cost_bh"], s["cost_rel"]))
+
+
 if __name__ == "__main__":
     main()
+    active_case()

@@ -38,7 +38,8 @@ def close(a, b):
 
 def test_fixtures_present():
     assert sorted(os.path.basename(p) for p in glob.glob(os.path.join(HERE, "*.npz"))) == [
-        "duplicates_630.npz", "lattice_512.npz", "massless_600.npz", "sheet_600.npz", "two_2.npz"]
+        "active_10pct_2000.npz", "duplicates_630.npz", "lattice_512.npz", "massless_600.npz", "sheet_600.npz",
+        "two_2.npz"]
 
 
 @pytest.mark.parametrize("name", ["sheet_600", "two_2", "lattice_512"])
@@ -89,3 +90,16 @@ def test_potential_walk_matches_reference(name):
     p = oracle.potential(g["pos"][k], g["mass"][k], g["h"][k], old_acc=g["oldacc_pot"],
                          err_tol_force_acc=float(g["tol"]))
     assert np.allclose(p, g["pot_only"], rtol=1e-12, atol=1e-14 * np.abs(g["pot_only"]).max())
+
+
+def test_active_subset_matches_reference():
+    """GIZMO walks only the active particles on a tree of all of them; the
+    Barnes-Hut pass gives the active ones their OldAcc for the relative pass."""
+    g = load("active_10pct_2000")
+    act, tol = g["active"], float(g["tol"])
+    a1, p1, _, c1 = oracle.tree_gravity(g["pos"], g["mass"], g["h"], None, tol, 0.7, targets=act)
+    old = np.zeros(g["pos"].shape[0])
+    old[act] = np.linalg.norm(a1, axis=1)
+    a2, p2, _, c2 = oracle.tree_gravity(g["pos"], g["mass"], g["h"], old, tol, 0.0, targets=act)
+    assert c1 == int(g["cost_bh"]) and c2 == int(g["cost_rel"])
+    assert close(a1, g["acc_bh"]) and close(a2, g["acc"]) and close(p2, g["pot"])
