@@ -20,6 +20,9 @@ interaction counter is exact) on two seeded 600-particle Plummer spheres:
       seeded 10% are active: both start-up passes walk only those (the
       harness's sample-only mode sets GIZMO's active list), with the tree
       built from all particles.
+  active_drift_2000: the same system, all particles active at start-up,
+      then a drift of DRIFT_DT without a rebuild after which only a seeded
+      10% are active (force_drift_node inside the reference's walk).
 
 Stores the inputs, the reference's Barnes-Hut and relative passes (GravAccel,
 Potential with G = 1, interaction counts), the potential-only walk
@@ -41,6 +44,7 @@ import ics  # noqa: E402
 import ref_runner  # noqa: E402
 
 TOL = 0.0025
+DRIFT_DT = 0.005
 
 
 def cases():
@@ -91,6 +95,19 @@ def active_case():
     print("active_10pct_2000 active=%d cost_bh=%d cost_rel=%d" % (act.size, s["cost_bh"], s["cost_rel"]))
 
 
+def active_drift_case():
+    ic = ics.clustered(2000, seed=231, n_clumps=10)
+    act = ics.random_active(2000, 0.1, seed=233)
+    r = ref_runner.run(ic, tol=TOL, threads=1, sample=act, drift_dt=DRIFT_DT)
+    dr = r["info"]["drift"]
+    np.savez_compressed(
+        os.path.join(HERE, "active_drift_2000.npz"), pos=ic["pos"], vel=ic["vel"], mass=ic["mass"], h=ic["h"],
+        tol=TOL, active=act, drift_dt=dr["dt"], pos_drift=r["pos_drift"][act], acc_drift=r["acc_drift"][act],
+        pot_drift=r["pot_drift"][act], cost_drift=dr["cost"])
+    print("active_drift_2000 active=%d cost_drift=%d" % (act.size, dr["cost"]))
+
+
 if __name__ == "__main__":
     main()
     active_case()
+    active_drift_case()

@@ -38,7 +38,7 @@ def close(a, b):
 
 def test_fixtures_present():
     assert sorted(os.path.basename(p) for p in glob.glob(os.path.join(HERE, "*.npz"))) == [
-        "active_10pct_2000.npz", "duplicates_630.npz", "lattice_512.npz", "massless_600.npz", "sheet_600.npz",
+        "active_10pct_2000.npz", "active_drift_2000.npz", "duplicates_630.npz", "lattice_512.npz", "massless_600.npz", "sheet_600.npz",
         "two_2.npz"]
 
 
@@ -103,3 +103,18 @@ def test_active_subset_matches_reference():
     a2, p2, _, c2 = oracle.tree_gravity(g["pos"], g["mass"], g["h"], old, tol, 0.0, targets=act)
     assert c1 == int(g["cost_bh"]) and c2 == int(g["cost_rel"])
     assert close(a1, g["acc_bh"]) and close(a2, g["acc"]) and close(p2, g["pot"])
+
+
+def test_active_subset_after_drift_matches_reference():
+    """Start-up passes over all particles, then a drift without a rebuild and
+    a walk of the active 10% only: nodes drifted inside the walk
+    (force_drift_node) and the relative criterion on the start-up OldAcc."""
+    g = load("active_drift_2000")
+    act, tol = g["active"], float(g["tol"])
+    a1, _, _, _ = oracle.tree_gravity(g["pos"], g["mass"], g["h"], None, tol, 0.7)
+    a2, _, _, _ = oracle.tree_gravity(g["pos"], g["mass"], g["h"], np.linalg.norm(a1, axis=1), tol, 0.0)
+    a3, p3, _, c3, moved = oracle.tree_gravity_drift(g["pos"], g["vel"], g["mass"], g["h"], float(g["drift_dt"]),
+                                                     np.linalg.norm(a2, axis=1), tol, 0.0, targets=act)
+    assert c3 == int(g["cost_drift"])
+    assert np.allclose(moved[act], g["pos_drift"], rtol=0, atol=4 * np.spacing(np.abs(g["pos_drift"]).max()))
+    assert close(a3, g["acc_drift"]) and close(p3, g["pot_drift"])
