@@ -58,3 +58,56 @@ def test_invalid_arguments_rejected_without_device():
     cfg.node_staging = 2
     assert lib.gg_create(ctypes.byref(cfg), ctypes.byref(h)) == -1
     assert lib.gg_radix_sort_pairs(-1, None, None, 64, None) == -1
+
+
+def _header_struct(name):
+    """(type, field, count) of `typedef struct name { ... } name;` in the public header."""
+    import re
+    here = os.path.dirname(ggb200.__file__)
+    text = open(os.path.join(here, "..", "include", "gizmo_gravity_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (name, name), text, flags=re.S).group(1)
+    out = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        m = re.match(r"(\w+)\s+(\w+)(?:\[(\d+)\])?$", decl)
+        assert m, decl
+        out.append((m.group(1), m.group(2), int(m.group(3) or 1)))
+    return out
+
+
+C_TYPES = {"int32_t": ctypes.c_int32, "int64_t": ctypes.c_int64, "double": ctypes.c_double}
+
+
+def _mirror(fields):
+    out = []
+    for name, t in fields:
+        if hasattr(t, "_length_"):   # array: element type and count
+            out.append((t._type_, name, t._length_))
+        else:
+            out.append((t, name, 1))
+    return out
+
+
+def test_binding_structs_mirror_header():
+    for cname, py in (("gg_config", ggb200.Config), ("gg_stats", ggb200.Stats), ("gg_domain", ggb200.Domain)):
+        h = _header_struct(cname)
+        m = _mirror(py._fields_)
+        assert [f for _, f, _ in h] == [f for _, f, _ in m], cname
+        for (ct, f, n), (pt, _, pn) in zip(h, m):
+            assert ctypes.sizeof(C_TYPES[ct]) == ctypes.sizeof(pt) and n == pn, (cname, f)
+
+
+def test_particle_record_layout():
+    import numpy as np
+    dt = ggb200.PART_DTYPE
+    assert dt.itemsize == 32
+    assert [(k, dt.fields[k][1]) for k in ("x", "y", "z", "m", "h")] == [("x", 0), ("y", 8), ("z", 16), ("m", 24),
+                                                                         ("h", 28)]
+    pos = np.arange(12, dtype=np.float64).reshape(4, 3) + 0.1
+    rec = ggb200.make_records(pos, np.full(4, 0.25), np.full(4, 0.028))
+    assert np.array_equal(np.stack([rec["x"], rec["y"], rec["z"]], 1), pos)
+    assert rec["m"].dtype == np.float32 and np.all(rec["m"] == np.float32(0.25))
+    assert np.all(rec["h"] == np.float32(0.028))
