@@ -5,8 +5,11 @@ A step is one pass of the hot path over one system held in HBM: root cube,
 Peano-Hilbert keys, radix sort, permutation, oct-tree build with FP64 moments,
 and the relative-criterion walk (ErrTolForceAcc, OldAcc left on the device by
 the previous step) -- what every GIZMO step pays when the tree is rebuilt.
-The default workload is the 4,194,304-particle galaxy (Hernquist halo +
-exponential disk).  Inputs are larger than L2 (no flush needed).
+The default workload is the 16,777,216-particle clustered system (1,000
+Plummer clumps with log-normal masses plus a 20% uniform background), all
+particles active; the same run also times a full rebuild plus the walk of a
+seeded random 10% of the targets (individual timesteps).  Inputs are larger
+than L2 (no flush needed).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -21,6 +24,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -38,6 +42,8 @@ FLOPS_PER_INTERACTION = 20   # monopole force convention (3 sub, r^2, rsqrt, m/r
 # written); the walk's traffic grows with the particle count, so a launch of
 # the 4.2M galaxy is scaled from it
 WALK_DRAM_BYTES_PER_PARTICLE = {"galaxy": 154.4, "galaxy1m": 154.4}
+WALK_DRAM_SOURCE = {k: "ncu dram bytes of one k_walk launch on the 1M galaxy, scaled by N"
+                    for k in WALK_DRAM_BYTES_PER_PARTICLE}
 METRIC = "tree-gravity particles/s at p99 force err<=2e-3 vs FP64 direct; serve p50/p99 ms"
 
 WORKLOADS = {
@@ -66,11 +72,10 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % index)
+        self.path = os.path.join(tempfile.gettempdir(), "gg_bench_clocks_%d_%d.csv" % (os.getpid(), index))
 
     def start(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
                                           "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
@@ -150,9 +155,89 @@ def cpu_reference_rate(ic, seconds=15.0, seed=1, tol=0.0025, active_n=None):
             "t_build_s": t_build, "t_walk_per_particle_us": per * 1e6}
 
 
+REF_BLOCKS, REF_BLOCK_LEN = 64, 1024   # PH-contiguous sample of the reference timing: 64 runs of 1,024 targets
+REF_FULL_MAX = 262144                   # systems up to this size are walked whole by the reference
+
+
+def reference_sample(ic, seed=1):
+    """Targets the reference is timed on, as GIZMO walks them: the whole
+    system when it is small, else runs of 1,024 particles consecutive in
+    Peano-Hilbert order at seeded places along the curve (64 runs of 1,024)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_runner
+    n = ic["pos"].shape[0]
+    if n <= REF_FULL_MAX:
+        return np.arange(n), "all %d targets" % n
+    smp = ref_runner.ph_block_sample(ic["pos"], REF_BLOCKS, REF_BLOCK_LEN, seed=seed)
+    return smp, "%d runs of %d targets consecutive in Peano-Hilbert order" % (REF_BLOCKS, REF_BLOCK_LEN)
+
+
+def cpu_reference(ic, ref_tg, args, n_eval):
+    """The reference (compiled GIZMO, OpenMP, all host threads) on this
+    system, two bounded runs: (1) its forces on the sampled targets `ref_tg`
+    (random), with their walk time; (2) its timing on a Peano-Hilbert
+    contiguous sample, the order GIZMO's own walk takes.  Each run times one
+    rebuild (domain_Decomposition + tree build) and one walk of its sample on
+    the resident tree.  Returns (cpu_baseline, reference results on ref_tg);
+    the C restatement stands in, without forces, where the compiled reference
+    cannot run."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_runner
+    if not ref_runner.available():
+        return cpu_reference_rate(ic, seconds=args.cpu_seconds, tol=args.tol, active_n=n_eval), None
+    n = ic["pos"].shape[0]
+    r_rand, i_rand = ref_runner.steps_rate(ic, steps=1, warmup=0, sample=ref_tg, tol=args.tol, active_n=n_eval,
+                                           sample_kind="%d seeded random targets" % ref_tg.size)
+    smp, kind = reference_sample(ic)
+    if smp.size == n:
+        r_ph, i_ph = r_rand, i_rand
+        if ref_tg.size != n:
+            r_ph, i_ph = ref_runner.steps_rate(ic, steps=1, warmup=0, sample=smp, tol=args.tol, active_n=n_eval,
+                                               sample_kind=kind)
+    else:
+        r_ph, i_ph = ref_runner.steps_rate(ic, steps=1, warmup=0, sample=smp, tol=args.tol, active_n=n_eval,
+                                           sample_kind=kind)
+    v_ph, v_rand = float(np.mean(r_ph)), float(np.mean(r_rand))
+    cpu = {"value": v_ph, "unit": "particles/s", "cores": i_ph["cores"], "kind": "reference",
+           "sample": i_ph["sample"], "t_domain_s": i_ph["t_domain_s"], "t_build_s": i_ph["t_build_s"],
+           "t_walk_per_particle_us": i_ph["t_walk_per_particle_us"], "timed_walk_s": i_ph["step_s"],
+           "t_walk_fixed_s": i_ph["t_walk_fixed_s"], "t_empty_walk_s": i_ph["t_empty_walk_s"],
+           "model": "n / (t_domain + t_build + t_walk_fixed + t_walk_per_particle x n)",
+           "random_sample": {"value": v_rand, "sample": i_rand["sample"],
+                             "t_walk_per_particle_us": i_rand["t_walk_per_particle_us"]},
+           "random_over_ph_blocks": v_rand / v_ph, "host_cpu": host_cpu()}
+    res = {"acc": i_rand["acc"], "pot": i_rand["pot"]}
+    return cpu, res
+
+
+def subset_reference_rate(cpu, n_sub):
+    """The reference's targets/s for a step that rebuilds and walks n_sub
+    targets, from the same measured rebuild and per-target walk time."""
+    per = cpu["t_walk_per_particle_us"] * 1e-6
+    t = cpu["t_domain_s"] + cpu["t_build_s"] + cpu.get("t_walk_fixed_s", 0.0) + per * n_sub
+    return {"value": n_sub / t, "unit": "targets/s",
+            "cores": cpu["cores"], "kind": cpu["kind"],
+            "sample": "the all-active run's measured rebuild and walk time per target (%s)" % cpu["sample"]}
+
+
+def host_cpu():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return "%s x %d" % (line.split(":", 1)[1].strip(), os.cpu_count() or 1)
+    except OSError:
+        pass
+    return None
+
+
 def run_reference_arm(args):
-    """Time the reference's own CPU tree gravity (all host threads) on this
-    arm's workload: W+K steady-state steps, each a bounded sample of targets."""
+    """Time the reference's own CPU tree gravity (compiled GIZMO, OpenMP, all
+    host threads) on this arm's workload.  Small systems: W+K whole steps
+    (domain_Decomposition + tree build + relative walk of every particle).
+    Large systems: one measured rebuild, then W+K timed walks of a bounded
+    Peano-Hilbert contiguous sample of targets on the resident tree; `value` is
+    the modelled rate of a whole step from those measured parts, and
+    `ms_per_step` the timed sample steps' own mean duration."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -163,26 +248,64 @@ def run_reference_arm(args):
     n = ic["pos"].shape[0]
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref_runner
-    if ref_runner.available():
-        active_n = int(round(args.active_frac * n)) if args.active_frac < 1.0 else None
-        rates, info = ref_runner.steps_rate(ic, steps=args.steps, warmup=args.warmup, sample_n=args.ref_sample,
-                                            tol=args.tol, active_n=active_n)
-        v = float(np.mean(rates))
-    else:
+    active_n = int(round(args.active_frac * n)) if args.active_frac < 1.0 else None
+    if not ref_runner.available():
         vals = [cpu_reference_rate(ic, seconds=args.ref_seconds, seed=1000 + i, tol=args.tol)
                 for i in range(args.warmup + args.steps)][args.warmup:]
         v = float(np.mean([x["value"] for x in vals]))
         info = vals[-1]
+        step_ms, extra = 1e3 * n / v, {}
+    else:
+        smp, kind = reference_sample(ic)
+        whole = smp.size == n and active_n is None
+        rates, info = ref_runner.steps_rate(ic, steps=args.steps, warmup=args.warmup, sample=smp, tol=args.tol,
+                                            active_n=active_n, rebuild_steps="all" if whole else 1, sample_kind=kind)
+        v = float(np.mean(rates))
+        step_ms = 1e3 * float(np.mean(info["step_s"]))
+        extra = {"timed_step": "whole step (domain + build + walk of every particle)" if whole else
+                 "walk of the sample on the resident tree (the rebuild is timed once and enters the model)",
+                 "model": "n / (t_domain + t_build + t_walk_fixed + t_walk_per_particle x n)",
+                 "t_domain_s": info["t_domain_s"], "t_build_s": info["t_build_s"],
+                 "t_walk_fixed_s": info["t_walk_fixed_s"], "t_empty_walk_s": info["t_empty_walk_s"],
+                 "t_walk_per_particle_us": info["t_walk_per_particle_us"],
+                 "model_ms_per_full_step": 1e3 * n / v if active_n is None else 1e3 * active_n / v}
+        if args.calibrate:
+            extra["calibration"] = reference_calibration(ic, args, active_n, v, kind)
     out = {"metric": METRIC, "value": v, "unit": "particles/s", "n_gpus": args.gpus, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": 1e3 * n / v, "higher_is_better": True, "scaling": "weak",
+           "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": name, "n": n, "err_tol_force_acc": args.tol},
+           "config": {"workload": name, "n": n, "err_tol_force_acc": args.tol,
+                      "active": active_n if active_n is not None else n},
            "impl": "reference",
            "cpu_baseline": {"value": v, "unit": "particles/s", "cores": info["cores"], "kind": info["kind"],
-                            "sample": info["sample"]},
+                            "sample": info["sample"], "host_cpu": host_cpu()},
            "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    out.update(extra)
     print(json.dumps(out), flush=True)
     return 0
+
+
+def reference_calibration(ic, args, active_n, v_main, kind_main):
+    """The same reference rate from other target samples: seeded random
+    targets, and (small systems) a Peano-Hilbert block sample beside the whole
+    step, so that the sample model can be checked against a full walk."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_runner
+    n = ic["pos"].shape[0]
+    out = {"main": {"value": v_main, "sample": kind_main}}
+    r, i = ref_runner.steps_rate(ic, steps=2, warmup=0, sample=min(16384, n // 4), tol=args.tol, active_n=active_n)
+    out["random"] = {"value": float(np.mean(r)), "sample": i["sample"],
+                     "t_walk_per_particle_us": i["t_walk_per_particle_us"]}
+    if n <= REF_FULL_MAX:
+        smp = ref_runner.ph_block_sample(ic["pos"], 4, 1024, seed=3)
+        r, i = ref_runner.steps_rate(ic, steps=2, warmup=0, sample=smp, tol=args.tol, active_n=active_n,
+                                     sample_kind="4 runs of 1,024 targets consecutive in Peano-Hilbert order")
+        out["ph_blocks"] = {"value": float(np.mean(r)), "sample": i["sample"],
+                            "t_walk_per_particle_us": i["t_walk_per_particle_us"]}
+    for k in list(out):
+        if k != "main":
+            out[k]["over_main"] = out[k]["value"] / v_main
+    return out
 
 
 # ---------------------------------------------------------------- batched ensemble
@@ -235,7 +358,7 @@ def systems_reference_rate(systems, tol, what):
     for sub in systems:
         n = int(sub["pos"].shape[0])
         try:
-            rates, info = ref_runner.steps_rate(sub, steps=1, warmup=0, sample_n=n, tol=tol)
+            rates, info = ref_runner.steps_rate(sub, steps=1, warmup=0, sample=n, tol=tol, rebuild_steps="all")
         except RuntimeError as e:
             # the reference's own limits can end a run (e.g. its top-node
             # allocation in force_create_empty_nodes on a small system): that
@@ -654,6 +777,311 @@ def run_reference_arm_systems(args):
     return 0
 
 
+# ---------------------------------------------------------------- one system per GPU
+def timed_steps(torch, stream, tree, walk, steps):
+    """`steps` steps of build + walk between two CUDA events on the library's
+    stream, with an event between build and walk.  Returns (total ms, mean
+    build ms, mean walk ms)."""
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * steps + 1)]
+    ev[0].record(stream)
+    for k in range(steps):
+        tree.build()
+        ev[2 * k + 1].record(stream)
+        walk()
+        ev[2 * k + 2].record(stream)
+    torch.cuda.synchronize()
+    total = ev[0].elapsed_time(ev[-1])
+    walk_ms = sum(ev[2 * k + 1].elapsed_time(ev[2 * k + 2]) for k in range(steps)) / steps
+    build_ms = sum(ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(steps)) / steps
+    return total, build_ms, walk_ms
+
+
+def sample_w(mass, pot):
+    """1/2 sum m phi over a sample of targets."""
+    return 0.5 * float(np.sum(mass * pot))
+
+
+def reference_errors(ref, acc_dir, pot_dir, mass, acc_gpu, pot_gpu):
+    """The reference tree's and this walk's errors on the same targets."""
+    r50, r99, _ = ics.error_stats(ref["acc"], acc_dir)
+    g50, g99, _ = ics.error_stats(acc_gpu, acc_dir)
+    w_dir, w_ref, w_gpu = sample_w(mass, pot_dir), sample_w(mass, ref["pot"]), sample_w(mass, pot_gpu)
+    return {"targets": int(acc_dir.shape[0]), "p50": g50, "p99": g99, "ref_p50": r50, "ref_p99": r99,
+            "p50_vs_ref": g50 / r50, "p99_vs_ref": g99 / r99,
+            "within_1p1_of_reference": bool(g50 <= 1.1 * r50 and g99 <= 1.1 * r99),
+            "W_rel_err": abs(w_gpu - w_dir) / abs(w_dir), "ref_W_rel_err": abs(w_ref - w_dir) / abs(w_dir),
+            "W_rel_diff_vs_ref": abs(w_gpu - w_ref) / abs(w_ref),
+            "W_no_worse_than_ref_or_1e-5": bool(abs(w_gpu - w_dir) <= max(abs(w_ref - w_dir), 1e-5 * abs(w_dir))),
+            "W": "1/2 sum m phi over these targets"}
+
+
+def run_system(args, torch, ggb200, dist, world, rank, local):
+    """One system per GPU (independent seeded systems per rank: weak scaling).
+    A step = build (extent, keys, sort, permute, tree, moments) + relative walk
+    of every particle, OldAcc left on the device by the previous step.  With
+    --subset-frac (default 0.1 on the clustered system) a second timed loop
+    walks a seeded random subset of targets on a full rebuild (individual
+    timesteps), reported in the same line."""
+    name, gen = WORKLOADS[args.workload]
+    ic = gen(multi.rank_seed(SEEDS[args.workload], rank))   # independent system per rank
+    n = ic["pos"].shape[0]
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)   # every kernel and event of the bench goes on this stream
+    torch.cuda.set_stream(stream)
+    rec = ggb200.make_records(ic["pos"], ic["mass"], ic["h"])
+    d_rec = torch.from_numpy(rec.view(np.uint8)).to(dev)
+    d_acc = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    d_pot = torch.empty(n, dtype=torch.float64, device=dev)
+
+    kw = dict(leaf_size=args.leaf, group_size=args.group, flush=args.flush, device=local,
+              blocks_per_sm=args.blocks_per_sm, target_order=args.target_order, group_order=args.group_order,
+              node_staging=args.node_staging)
+    tree = ggb200.GravityTree(**kw)
+    tree.set_stream(stream.cuda_stream)
+    tree.load_device(d_rec, [n])
+    # start-up Barnes-Hut pass gives OldAcc (accel.c:47-50), then one relative
+    # pass over all particles: every later step starts from a relative walk's
+    # OldAcc, left on the device
+    tree.build()
+    tree.evaluate_device(d_acc, d_pot, err_tol_theta=0.7)
+    tree.build()
+    tree.evaluate_device(d_acc, d_pot, err_tol_force_acc=args.tol, err_tol_theta=0.0)
+
+    act, d_act, na = None, None, n
+    if args.active_frac < 1.0:
+        act = ics.random_active(n, args.active_frac, seed=multi.rank_seed(77, rank)).astype(np.int32)
+        na = int(act.size)
+        d_act = torch.from_numpy(act).to(dev)
+
+    def walker(t, d_a, n_a, acc_out, pot_out):
+        def walk():
+            if args.potential:
+                t.evaluate_potential_device(pot_out, d_active=d_a, n_active=n_a, err_tol_force_acc=args.tol,
+                                            err_tol_theta=0.0)
+            else:
+                t.evaluate_device(acc_out, pot_out, d_active=d_a, n_active=n_a, err_tol_force_acc=args.tol,
+                                  err_tol_theta=0.0)
+        return walk
+
+    walk = walker(tree, d_act, na if act is not None else 0, d_acc, d_pot)
+    for _ in range(args.warmup):
+        tree.build()
+        walk()
+    torch.cuda.synchronize()
+    if tree.last_stats()["error_word"]:
+        raise RuntimeError("device error word %d" % tree.last_stats()["error_word"])
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = ggb200.kernel_launches()
+    total_ms, build_ms, walk_ms = timed_steps(torch, stream, tree, walk, args.steps)
+    if dist:
+        dist.barrier()
+    launches = ggb200.kernel_launches() - launches0
+    clk = clocks.stop()
+    total_ms = multi.max_over_ranks(dist, total_ms, device=dev)
+    n_all = multi.sum_over_ranks(dist, na, device=dev)   # targets evaluated per step
+    stats = tree.last_stats()
+    if stats["error_word"]:
+        raise RuntimeError("device error word %d in the timed steps" % stats["error_word"])
+    ms_step = total_ms / args.steps
+    value = n_all / (ms_step * 1e-3)
+    inter = stats["interactions"]
+    acc = d_acc[:na].cpu().numpy()
+    pot = d_pot[:na].cpu().numpy()
+
+    # individual timesteps: a random subset of targets walked on a full rebuild,
+    # from the all-particle OldAcc the timed steps left (same for every rank)
+    subset = None
+    if args.subset_frac > 0 and act is None:
+        sub = ics.random_active(n, args.subset_frac, seed=multi.rank_seed(77, rank)).astype(np.int32)
+        d_sub = torch.from_numpy(sub).to(dev)
+        d_acc_s = torch.empty((sub.size, 3), dtype=torch.float64, device=dev)
+        d_pot_s = torch.empty(sub.size, dtype=torch.float64, device=dev)
+        walk_s = walker(tree, d_sub, int(sub.size), d_acc_s, d_pot_s)
+        for _ in range(args.warmup):
+            tree.build()
+            walk_s()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        clocks_s = ClockSampler(local)
+        clocks_s.start()
+        time.sleep(0.3)
+        tot_s, build_s, walk_s_ms = timed_steps(torch, stream, tree, walk_s, args.steps)
+        clk_s = clocks_s.stop()
+        tot_s = multi.max_over_ranks(dist, tot_s, device=dev)
+        n_sub_all = multi.sum_over_ranks(dist, int(sub.size), device=dev)
+        st_s = tree.last_stats()
+        if st_s["error_word"]:
+            raise RuntimeError("device error word %d in the subset steps" % st_s["error_word"])
+        subset = {"active": int(sub.size), "fraction": args.subset_frac, "value": n_sub_all / (tot_s / args.steps * 1e-3),
+                  "unit": "targets/s", "ms_per_step": tot_s / args.steps, "build_ms": build_s, "walk_ms": walk_s_ms,
+                  "interactions_per_target": st_s["interactions"] / sub.size, "clocks": clk_s,
+                  "step": "full rebuild + relative walk of a seeded random %g of the particles" % args.subset_frac,
+                  "_targets": sub, "_acc": d_acc_s.cpu().numpy(), "_pot": d_pot_s.cpu().numpy()}
+        del d_acc_s, d_pot_s
+
+    # stage breakdown on one extra instrumented step (outside the timed region)
+    tprof = ggb200.GravityTree(timing=True, **kw)
+    tprof.set_stream(stream.cuda_stream)
+    tprof.load_device(d_rec, [n])
+    tprof.build()
+    tprof.evaluate_device(d_acc, d_pot, err_tol_theta=0.7)
+    # one relative walk first, so that the measured step starts, like the timed
+    # steps, from a relative walk's OldAcc and group costs
+    tprof.build()
+    tprof.evaluate_device(d_acc, d_pot, err_tol_force_acc=args.tol, err_tol_theta=0.0)
+    tprof.build()
+    walker(tprof, d_act, na if act is not None else 0, d_acc, d_pot)()
+    stages = tprof.last_stats()
+    tprof.close()
+
+    # force errors against the FP64 direct sum: a seeded sample of the outputs,
+    # plus the targets the reference tree is run on (a seeded sample of the
+    # subset, or of the active set), so that both trees are compared on the
+    # same targets
+    ne = min(args.err_targets, na)
+    rows = np.sort(np.random.default_rng(12345).choice(na, ne, replace=False))   # rows of the outputs
+    tg = (rows if act is None else act[rows]).astype(np.int32)                   # their particles
+    pool = subset["_targets"] if subset else (act if act is not None else np.arange(n, dtype=np.int32))
+    nref = min(args.ref_sample, pool.size)
+    ref_pick = np.sort(np.random.default_rng(2468).choice(pool.size, nref, replace=False))
+    ref_tg = pool[ref_pick].astype(np.int32)
+    all_tg = np.concatenate([tg, ref_tg])
+    dp = torch.from_numpy(ic["pos"]).to(dev)
+    dm = torch.from_numpy(ic["mass"]).to(dev)
+    dh = torch.from_numpy(ic["h"]).to(dev)
+    dacc = torch.empty((all_tg.size, 3), dtype=torch.float64, device=dev)
+    dpot = torch.empty(all_tg.size, dtype=torch.float64, device=dev)
+    ggb200.direct_sum_fp64(dp, dm, dh, n, torch.from_numpy(all_tg).to(dev), all_tg.size, dacc, dpot,
+                           stream.cuda_stream)
+    torch.cuda.synchronize()
+    acc_all_dir, pot_all_dir = dacc.cpu().numpy(), dpot.cpu().numpy()
+    del dp, dm, dh, dacc, dpot
+    acc_dir, pot_dir = acc_all_dir[:ne], pot_all_dir[:ne]
+    acc_rdir, pot_rdir = acc_all_dir[ne:], pot_all_dir[ne:]
+    if args.potential:   # the potential walk's own error: |phi - phi_direct| / |phi_direct|
+        e = np.abs(pot[rows] - pot_dir) / np.maximum(np.abs(pot_dir), 1e-300)
+        p50, p99 = float(np.median(e)), float(np.percentile(e, 99))
+    else:
+        p50, p99, _ = ics.error_stats(acc[rows], acc_dir)
+    force_error = {"p50": p50, "p99": p99, "targets": ne, "vs": "FP64 direct sum (GPU, same pair rule)",
+                   "W_rel_err_sample": abs(sample_w(ic["mass"][tg], pot[rows]) - sample_w(ic["mass"][tg], pot_dir))
+                   / abs(sample_w(ic["mass"][tg], pot_dir))}
+
+    # FP32 roofline of the walk (measured FMA peak on this GPU)
+    peak32 = ggb200.fp32_peak_tflops(stream.cuda_stream)
+    walk_tflops = inter * FLOPS_PER_INTERACTION / (stages["ms_walk"] * 1e-3) / 1e12 if stages["ms_walk"] else None
+    walk_phase_tflops = inter * FLOPS_PER_INTERACTION / (walk_ms * 1e-3) / 1e12
+
+    # HBM roofline of the sort (200 B per element: 8 passes x 24 B + 8 B histogram read)
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        hbm_peak, hbm_src = float(peaks["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
+    except Exception:
+        hbm_peak, hbm_src = 6650.0, "fallback 6.65 TB/s"
+    sort_gbs = 200.0 * n / (stages["ms_sort"] * 1e-3) / 1e9 if stages["ms_sort"] else None
+
+    # end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e and rank == 0:
+        old = np.linalg.norm(acc, axis=1) if act is None else torch.linalg.norm(
+            tree_all_acc(tree, torch, dev, n, args.tol), dim=1).cpu().numpy()
+        with ggb200.GravityTree(**kw) as te:
+            out = (np.empty((na, 3)), np.empty(na))   # the caller's result arrays, reused every step
+
+            def e2e_step():
+                te.load(ic["pos"], ic["mass"], ic["h"])
+                te.build()
+                return te.evaluate(active=act, old_acc=old, err_tol_force_acc=args.tol, out=out)
+            for _ in range(2):
+                e2e_step()
+            t0 = time.perf_counter()
+            ke = max(3, min(args.steps, 5))
+            for _ in range(ke):
+                e2e_step()
+            dt = (time.perf_counter() - t0) / ke
+        e2e = {"value": na / dt, "unit": "particles/s",
+               "h2d_bytes_per_step": int(n * (32 + 8) + (4 * na if act is not None else 0)),
+               "d2h_bytes_per_step": int(na * (24 + 8)), "ms_per_step": dt * 1e3,
+               "path": "gg_load_particles (host FP64 arrays) + gg_build + gg_evaluate (host outputs, OldAcc in)"}
+
+    # the reference tree (compiled GIZMO, host cores) on the same system: its
+    # forces on the sampled targets, and its timing, from two bounded runs
+    cpu, ref_cmp, sub_cmp = None, None, None
+    if not args.no_cpu and rank == 0 and world == 1 and not args.potential:
+        cpu, ref_res = cpu_reference(ic, ref_tg, args, n_eval=na)
+        if ref_res is not None:
+            ref_rows = np.searchsorted(act, ref_tg) if act is not None else ref_tg
+            ref_cmp = reference_errors(ref_res, acc_rdir, pot_rdir, ic["mass"][ref_tg], acc[ref_rows], pot[ref_rows])
+            if subset:
+                srows = np.searchsorted(subset["_targets"], ref_tg)
+                sub_cmp = reference_errors(ref_res, acc_rdir, pot_rdir, ic["mass"][ref_tg], subset["_acc"][srows],
+                                           subset["_pot"][srows])
+                subset["cpu_baseline"] = subset_reference_rate(cpu, subset["active"])
+    if ref_cmp:
+        force_error["vs_reference_tree"] = ref_cmp
+    if subset:
+        sp50, sp99, _ = ics.error_stats(subset["_acc"][np.searchsorted(subset["_targets"], ref_tg)], acc_rdir)
+        subset["force_error"] = sub_cmp or {"p50": sp50, "p99": sp99, "targets": int(ref_tg.size)}
+        for k in ("_targets", "_acc", "_pot"):
+            subset.pop(k)
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": name, "n": n, "active": na, "n_total": int(n_all), "err_tol_force_acc": args.tol,
+                   "walk": "potential only (compute_potential)" if args.potential else "force and potential",
+                   "step": "extent+keys+sort+permute+tree+moments+relative walk (OldAcc on device)",
+                   "l2": "inputs larger than L2 (32 B/particle records, %d MB + tree)" % (32 * n // 10 ** 6),
+                   "leaf_size": args.leaf, "group_size": args.group, "flush": args.flush,
+                   "group_order": "by previous walk's cost" if args.group_order else "target order",
+                   "node_staging": ["cp.async per lane", "bulk copies (TMA) per run"][args.node_staging],
+                   "parallelism": "independent system per GPU" if world > 1 else "1 GPU"},
+        "force_error": force_error,
+        "interactions_per_step": inter, "interactions_per_s": inter / (ms_step * 1e-3),
+        "interactions_per_particle": inter / na,
+        "stage_ms": {"keys": stages["ms_keys"], "sort": stages["ms_sort"], "build": stages["ms_build"],
+                     "walk": stages["ms_walk"], "timed_build_phase": build_ms, "timed_walk_phase": walk_ms},
+        "roofline": {"bound": "fp32", "kernel": "k_walk", "achieved": walk_tflops, "peak": peak32,
+                     "unit": "TFLOP/s", "frac": (walk_tflops / peak32) if walk_tflops else None,
+                     "traffic": (WALK_DRAM_BYTES_PER_PARTICLE[args.workload] * n
+                                 if args.workload in WALK_DRAM_BYTES_PER_PARTICLE else None),
+                     "traffic_source": WALK_DRAM_SOURCE.get(args.workload),
+                     "flops_per_interaction": FLOPS_PER_INTERACTION,
+                     "peak_source": "measured FP32 FMA probe (gg_fp32_peak_probe) on this GPU",
+                     "timed_phase_achieved": walk_phase_tflops},
+        "roofline_sort": {"bound": "hbm", "achieved": sort_gbs, "peak": hbm_peak, "unit": "GB/s",
+                          "frac": (sort_gbs / hbm_peak) if sort_gbs else None, "bytes_per_element": 200,
+                          "peak_source": hbm_src},
+        "clocks": clk, "gpu_launches": int(launches), "e2e": e2e, "cpu_baseline": cpu,
+    }
+    if subset:
+        out["active_subset"] = subset
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    tree.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def tree_all_acc(tree, torch, dev, n, tol):
+    """|a| of every particle from one relative walk of all of them (OldAcc for
+    the end-to-end leg when the timed walk covers a subset only)."""
+    d_a = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    tree.build()
+    tree.evaluate_device(d_a, None, err_tol_force_acc=tol, err_tol_theta=0.0)
+    torch.cuda.synchronize()
+    return d_a
+
+
 # ---------------------------------------------------------------- GPU arm
 def main():
     ap = argparse.ArgumentParser()
@@ -661,7 +1089,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="galaxy", choices=sorted(WORKLOADS) + ["ensemble", "serve"])
+    ap.add_argument("--workload", default="clustered", choices=sorted(WORKLOADS) + ["ensemble", "serve"])
     # ErrTolForceAcc; by default per workload, the largest of 0.001 and 0.0008
     # that keeps the p99 force error below 2e-3 (the metric's bound) with a margin:
     # at 0.001 the galaxy's p99 is 1.77e-3 but the clustered system's 2.0e-3
@@ -686,6 +1114,12 @@ def main():
     # individual timesteps: the timed walk evaluates a seeded random fraction of
     # the particles (the tree is still built over all of them)
     ap.add_argument("--active-frac", type=float, default=1.0)
+    # a second timed loop in the same run: full rebuild + walk of a seeded
+    # random fraction of the targets, reported as "active_subset" (default 0.1
+    # on the clustered system, 0 = none elsewhere)
+    ap.add_argument("--subset-frac", type=float, default=None)
+    # reference arm: also time the reference on other target samples
+    ap.add_argument("--calibrate", action="store_true")
     # one system shared by the ranks (strong scaling): each rank holds an equal
     # share, all-gathers the records each step and walks its own particles
     ap.add_argument("--split", action="store_true")
@@ -695,6 +1129,8 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.tol is None:
         args.tol = 0.0008 if args.workload.startswith("clustered") else 0.001
+    if args.subset_frac is None:
+        args.subset_frac = 0.1 if args.workload == "clustered" else 0.0
 
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -712,213 +1148,7 @@ def main():
     if args.split:
         return run_split(args, torch, ggb200, dist, world, rank, local)
 
-    name, gen = WORKLOADS[args.workload]
-    ic = gen(multi.rank_seed(SEEDS[args.workload], rank))   # independent system per rank
-    n = ic["pos"].shape[0]
-    dev = torch.device("cuda", local)
-    stream = torch.cuda.Stream(device=dev)   # every kernel and event of the bench goes on this stream
-    torch.cuda.set_stream(stream)
-    rec = ggb200.make_records(ic["pos"], ic["mass"], ic["h"])
-    d_rec = torch.from_numpy(rec.view(np.uint8)).to(dev)
-    d_acc = torch.empty((n, 3), dtype=torch.float64, device=dev)
-    d_pot = torch.empty(n, dtype=torch.float64, device=dev)
-
-    tree = ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush,
-                              device=local, blocks_per_sm=args.blocks_per_sm,
-                              target_order=args.target_order, group_order=args.group_order,
-                              node_staging=args.node_staging)
-    tree.set_stream(stream.cuda_stream)
-    tree.load_device(d_rec, [n])
-    # start-up Barnes-Hut pass gives OldAcc (accel.c:47-50), left on the device
-    tree.build()
-    tree.evaluate_device(d_acc, d_pot, err_tol_theta=0.7)
-    act, d_act, na = None, None, n
-    if args.active_frac < 1.0:
-        act = ics.random_active(n, args.active_frac, seed=multi.rank_seed(77, rank)).astype(np.int32)
-        na = int(act.size)
-        d_act = torch.from_numpy(act).to(dev)
-        # OldAcc of every particle from one relative pass over all of them
-        tree.build()
-        tree.evaluate_device(d_acc, d_pot, err_tol_force_acc=args.tol, err_tol_theta=0.0)
-
-    def walk(t):
-        if args.potential:
-            t.evaluate_potential_device(d_pot, d_active=d_act, n_active=na if act is not None else 0,
-                                        err_tol_force_acc=args.tol, err_tol_theta=0.0)
-        else:
-            t.evaluate_device(d_acc, d_pot, d_active=d_act, n_active=na if act is not None else 0,
-                              err_tol_force_acc=args.tol, err_tol_theta=0.0)
-
-    def step():
-        tree.build()
-        walk(tree)
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    st0 = tree.last_stats()
-    if st0["error_word"]:
-        raise RuntimeError("device error word %d" % st0["error_word"])
-
-    clocks = ClockSampler(local)
-    clocks.start()
-    time.sleep(0.3)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    launches0 = ggb200.kernel_launches()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 1)]
-    ev[0].record(stream)
-    for k in range(args.steps):
-        tree.build()
-        ev[2 * k + 1].record(stream)
-        walk(tree)
-        ev[2 * k + 2].record(stream)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    launches = ggb200.kernel_launches() - launches0
-    clk = clocks.stop()
-    total_ms = ev[0].elapsed_time(ev[-1])
-    walk_ms = sum(ev[2 * k + 1].elapsed_time(ev[2 * k + 2]) for k in range(args.steps)) / args.steps
-    build_ms = (ev[0].elapsed_time(ev[1]) + sum(ev[2 * k].elapsed_time(ev[2 * k + 1])
-                                                 for k in range(1, args.steps))) / args.steps
-    total_ms = multi.max_over_ranks(dist, total_ms, device=dev)
-    n_all = multi.sum_over_ranks(dist, na, device=dev)   # targets evaluated per step
-    stats = tree.last_stats()
-    ms_step = total_ms / args.steps
-    value = n_all / (ms_step * 1e-3)
-    inter = stats["interactions"]
-
-    # stage breakdown on one extra instrumented step (outside the timed region)
-    tprof = ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush, device=local,
-                               timing=True, blocks_per_sm=args.blocks_per_sm, target_order=args.target_order,
-                              group_order=args.group_order, node_staging=args.node_staging)
-    tprof.set_stream(stream.cuda_stream)
-    tprof.load_device(d_rec, [n])
-    tprof.build()
-    tprof.evaluate_device(d_acc, d_pot, err_tol_theta=0.7)
-    # one relative walk first, so that the measured step starts, like the timed
-    # steps, from a relative walk's OldAcc and group costs
-    tprof.build()
-    tprof.evaluate_device(d_acc, d_pot, err_tol_force_acc=args.tol, err_tol_theta=0.0)
-    tprof.build()
-    walk(tprof)
-    stages = tprof.last_stats()
-    tprof.close()
-
-    # force error against the FP64 direct sum on a seeded subsample
-    acc = d_acc[:na].cpu().numpy()
-    pot = d_pot[:na].cpu().numpy()
-    ne = min(args.err_targets, na)
-    rows = np.sort(np.random.default_rng(12345).choice(na, ne, replace=False))   # rows of the outputs
-    tg = (rows if act is None else act[rows]).astype(np.int32)                   # their particles
-    dp = torch.from_numpy(ic["pos"]).to(dev)
-    dm = torch.from_numpy(ic["mass"]).to(dev)
-    dh = torch.from_numpy(ic["h"]).to(dev)
-    dacc = torch.empty((ne, 3), dtype=torch.float64, device=dev)
-    dpot = torch.empty(ne, dtype=torch.float64, device=dev)
-    ggb200.direct_sum_fp64(dp, dm, dh, n, torch.from_numpy(tg).to(dev), ne, dacc, dpot,
-                           stream.cuda_stream)
-    torch.cuda.synchronize()
-    acc_dir, pot_dir = dacc.cpu().numpy(), dpot.cpu().numpy()
-    if args.potential:   # the potential walk's own error: |phi - phi_direct| / |phi_direct|
-        e = np.abs(pot[rows] - pot_dir) / np.maximum(np.abs(pot_dir), 1e-300)
-        p50, p99 = float(np.median(e)), float(np.percentile(e, 99))
-    else:
-        p50, p99, _ = ics.error_stats(acc[rows], acc_dir)
-    wsum = float(np.sum(ic["mass"][tg] * pot[rows]))
-    wsum_dir = float(np.sum(ic["mass"][tg] * pot_dir))
-    del dp, dm, dh, dacc, dpot
-
-    # FP32 roofline of the walk (measured FMA peak on this GPU)
-    peak32 = ggb200.fp32_peak_tflops(stream.cuda_stream)
-    walk_tflops = inter * FLOPS_PER_INTERACTION / (stages["ms_walk"] * 1e-3) / 1e12 if stages["ms_walk"] else None
-    walk_phase_tflops = inter * FLOPS_PER_INTERACTION / (walk_ms * 1e-3) / 1e12
-
-    # HBM roofline of the sort (200 B per element: 8 passes x 24 B + 8 B histogram read)
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-        hbm_peak, hbm_src = float(peaks["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
-    except Exception:
-        hbm_peak, hbm_src = 6650.0, "fallback 6.65 TB/s"
-    sort_gbs = 200.0 * n / (stages["ms_sort"] * 1e-3) / 1e9 if stages["ms_sort"] else None
-
-    # end to end through the public API with host buffers
-    e2e = None
-    if not args.no_e2e and rank == 0:
-        if act is None:
-            old = np.linalg.norm(acc, axis=1)
-        else:   # OldAcc of every particle: the device copy after one more full relative pass
-            tree.build()
-            tree.evaluate_device(d_acc, d_pot, err_tol_force_acc=args.tol, err_tol_theta=0.0)
-            old = torch.linalg.norm(d_acc, dim=1).cpu().numpy()
-        with ggb200.GravityTree(leaf_size=args.leaf, group_size=args.group, flush=args.flush,
-                                device=local, blocks_per_sm=args.blocks_per_sm,
-                              target_order=args.target_order, group_order=args.group_order,
-                              node_staging=args.node_staging) as te:
-            out = (np.empty((na, 3)), np.empty(na))   # the caller's result arrays, reused every step
-
-            def e2e_step():
-                te.load(ic["pos"], ic["mass"], ic["h"])
-                te.build()
-                return te.evaluate(active=act, old_acc=old, err_tol_force_acc=args.tol, out=out)
-            for _ in range(2):
-                e2e_step()
-            t0 = time.perf_counter()
-            ke = max(3, min(args.steps, 5))
-            for _ in range(ke):
-                e2e_step()
-            dt = (time.perf_counter() - t0) / ke
-        e2e = {"value": na / dt, "unit": "particles/s",
-               "h2d_bytes_per_step": int(n * (32 + 8) + (4 * na if act is not None else 0)),
-               "d2h_bytes_per_step": int(na * (24 + 8)), "ms_per_step": dt * 1e3,
-               "path": "gg_load_particles (host FP64 arrays) + gg_build + gg_evaluate (host outputs, OldAcc in)"}
-
-    cpu = None
-    if not args.no_cpu and rank == 0 and world == 1:
-        ic_cpu = dict(ic)
-        ic_cpu["acc_hint"] = acc
-        cpu = cpu_reference_rate(ic_cpu, seconds=args.cpu_seconds, tol=args.tol,
-                                 active_n=na if act is not None else None)
-
-    out = {
-        "metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": name, "n": n, "active": na, "n_total": int(n_all), "err_tol_force_acc": args.tol,
-                   "walk": "potential only (compute_potential)" if args.potential else "force and potential",
-                   "step": "extent+keys+sort+permute+tree+moments+relative walk (OldAcc on device)",
-                   "l2": "inputs larger than L2 (32 B/particle records, 134 MB + tree)",
-                   "leaf_size": args.leaf, "group_size": args.group, "flush": args.flush,
-                   "group_order": "by previous walk's cost" if args.group_order else "target order",
-                   "node_staging": ["cp.async per lane", "bulk copies (TMA) per run"][args.node_staging],
-                   "parallelism": "independent system per GPU" if world > 1 else "1 GPU"},
-        "force_error": {"p50": p50, "p99": p99, "targets": ne, "vs": "FP64 direct sum (GPU, same pair rule)",
-                        "pot_sum_rel_diff_sample": abs(wsum - wsum_dir) / abs(wsum_dir)},
-        "interactions_per_step": inter, "interactions_per_s": inter / (ms_step * 1e-3),
-        "interactions_per_particle": inter / na,
-        "stage_ms": {"keys": stages["ms_keys"], "sort": stages["ms_sort"], "build": stages["ms_build"],
-                     "walk": stages["ms_walk"], "timed_build_phase": build_ms, "timed_walk_phase": walk_ms},
-        "roofline": {"bound": "fp32", "kernel": "k_walk", "achieved": walk_tflops, "peak": peak32,
-                     "unit": "TFLOP/s", "frac": (walk_tflops / peak32) if walk_tflops else None,
-                     "traffic": (WALK_DRAM_BYTES_PER_PARTICLE[args.workload] * n
-                                 if args.workload in WALK_DRAM_BYTES_PER_PARTICLE else None),
-                     "traffic_source": "ncu dram bytes of one k_walk launch on the 1M galaxy, scaled by N",
-                     "flops_per_interaction": FLOPS_PER_INTERACTION,
-                     "peak_source": "measured FP32 FMA probe (gg_fp32_peak_probe) on this GPU",
-                     "timed_phase_achieved": walk_phase_tflops},
-        "roofline_sort": {"bound": "hbm", "achieved": sort_gbs, "peak": hbm_peak, "unit": "GB/s",
-                          "frac": (sort_gbs / hbm_peak) if sort_gbs else None, "bytes_per_element": 200,
-                          "peak_source": hbm_src},
-        "clocks": clk, "gpu_launches": int(launches), "e2e": e2e, "cpu_baseline": cpu,
-    }
-    if rank == 0:
-        print(json.dumps(out), flush=True)
-    tree.close()
-    if dist:
-        dist.destroy_process_group()
-    return 0
+    return run_system(args, torch, ggb200, dist, world, rank, local)
 
 
 if __name__ == "__main__":

@@ -141,10 +141,12 @@ def types_and_eps(h):
 
 
 def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeout=3600, binary=None,
-        sample_only=False, drift_dt=0.0):
+        sample_only=False, drift_dt=0.0, rebuild_steps=None):
     """Run the reference: start-up evaluation (BH pass, relative pass) and
-    optional steady-state steps.  Returns dict with acc (pre-G = acc/G with
-    G = 1), pot, oldacc in input order, interaction counts and timings."""
+    optional steady-state steps (the first `rebuild_steps` of them rebuild,
+    the others walk the resident tree again; default: all rebuild).  Returns
+    dict with acc (pre-G = acc/G with G = 1), pot, oldacc in input order,
+    interaction counts and timings."""
     pos, mass, h = ic["pos"], ic["mass"], ic["h"]
     vel = ic.get("vel", np.zeros_like(pos))
     n = pos.shape[0]
@@ -160,21 +162,16 @@ def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeou
         with open(os.path.join(d, "params"), "w") as f:
             f.write(PARAMS.format(ic=icp, out=os.path.join(d, "out"), memmb=memmb, eps1=repr(eps1), eps2=repr(eps2)))
         args = [binary or BIN, os.path.join(d, "params"), repr(tol), os.path.join(d, "res.bin")]
-        if steps or sample is not None or drift_dt > 0:
-            args.append(str(steps))
-            if sample is None and drift_dt > 0:
-                args += ["-", "0"]
+        if steps or sample is not None or drift_dt > 0 or rebuild_steps is not None:
+            sp = "-"
             if sample is not None:
                 sp = os.path.join(d, "sample.bin")
                 # IDs in the file are positions in the type-ordered file, plus one
                 inv = np.empty(n, np.int64)
                 inv[order] = np.arange(n)
                 (inv[np.asarray(sample)] + 1).astype("<i8").tofile(sp)
-                args.append(sp)
-                if sample_only or drift_dt > 0:
-                    args.append("1" if sample_only else "0")
-            if drift_dt > 0:
-                args.append(repr(float(drift_dt)))
+            args += [str(steps), sp, "1" if sample_only else "0", repr(float(drift_dt)),
+                     str(steps if rebuild_steps is None else int(rebuild_steps))]
         env = dict(os.environ)
         if threads:
             env["OMP_NUM_THREADS"] = str(threads)
@@ -222,6 +219,8 @@ def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeou
             if line.startswith("domain"):
                 kv = dict(p.split("=", 1) for p in line.split()[1:])
                 info["domain"] = {"corner": [float(x) for x in kv["corner"].split(",")], "len": float(kv["len"])}
+            if line.startswith("empty"):
+                info["empty_walk_s"] = float(line.split("=", 1)[1])
             if line.startswith("startup") or line.startswith("step"):
                 kv = dict(p.split("=", 1) for p in line.split()[1 if line.startswith("startup") else 2:] if "=" in p)
                 kv = {k: float(v) for k, v in kv.items()}
@@ -237,42 +236,91 @@ def run(ic, tol=0.0025, steps=0, sample=None, threads=None, workdir=None, timeou
             shutil.rmtree(d, ignore_errors=True)
 
 
-def steps_rate(ic, steps=3, warmup=1, sample_n=16384, seed=1, tol=0.0025, threads=None, active_n=None):
+def ph_block_sample(pos, n_blocks, block_len, seed=1):
+    """A sample of targets as GIZMO walks them: `n_blocks` runs of `block_len`
+    particles that are consecutive in Peano-Hilbert order (the order of P[]
+    after domain_Decomposition, in which the OpenMP walk hands out its active
+    particles), one run at a seeded random place in each of n_blocks equal
+    stretches of the curve.  Returns sorted particle indices."""
+    import oracle
+    n = pos.shape[0]
+    if n_blocks * block_len >= n:
+        return np.arange(n)
+    _, lo = oracle.ph_keys(pos, oracle.find_extent(pos), bits=21)
+    order = np.argsort(lo, kind="stable")
+    rng = np.random.default_rng(seed)
+    stretch = n // n_blocks
+    starts = np.arange(n_blocks) * stretch + rng.integers(0, max(stretch - block_len, 0) + 1, size=n_blocks)
+    return np.sort(np.concatenate([order[a:a + block_len] for a in starts]))
+
+
+def steps_rate(ic, steps=3, warmup=1, sample=16384, seed=1, tol=0.0025, threads=None, active_n=None,
+               rebuild_steps=1, sample_kind=None):
     """The reference's particles/s per steady-state step, from a bounded sample.
 
-    One run of GIZMO's own code: start-up passes on a seeded random sample of
-    targets, then warmup+steps steps of domain_Decomposition (keys, sort,
-    reorder), tree build and the relative walk of the sampled targets.  A
-    step's cost for all N particles is domain + build + (walk time per sampled
-    target) x N.  Returns (per-step rates of the timed steps, info)."""
+    One run of GIZMO's own code with only the sampled targets active: the
+    start-up passes (Barnes-Hut, then relative), then `rebuild_steps` steps of
+    domain_Decomposition (keys, sort, reorder) + tree build + relative walk,
+    then warmup + steps walks of the sample on the resident tree
+    (rebuild_steps="all": warmup + steps steps that each rebuild).  `sample` is
+    a count (seeded random targets) or an index array.  A step's cost for n_eval
+    targets is modelled as the measured rebuild (domain + build) plus the
+    measured walk time per sampled target times n_eval.  Returns (model rates
+    of the timed steps, info); info["step_s"] holds the timed steps' own
+    durations and info["acc"] the sample's start-up relative-pass forces."""
     n = ic["pos"].shape[0]
     cores = threads or os.cpu_count() or 1
-    ns = min(n, sample_n)
-    sample = np.sort(np.random.default_rng(seed).choice(n, ns, replace=False))
-    res = run(ic, tol=tol, steps=warmup + steps, sample=sample, threads=cores, sample_only=True)
+    if np.ndim(sample) == 0:
+        ns = min(n, int(sample))
+        sample = np.sort(np.random.default_rng(seed).choice(n, ns, replace=False))
+        sample_kind = sample_kind or "%d seeded random targets" % ns
+    sample = np.asarray(sample)
+    ns = sample.size
     n_eval = n if active_n is None else int(active_n)   # targets a step evaluates
-    rates, per_list = [], []
-    for st in res["info"]["steps"][warmup:]:
-        per = max(st["t_gravity"] - st["t_build"], 1e-12) / ns
-        rates.append(n_eval / (st["t_domain"] + st["t_build"] + per * n_eval))
-        per_list.append(per)
-    last = res["info"]["steps"][-1]
+    fixed = 0.0
+    if rebuild_steps == "all":   # every step rebuilds: each timed step is a whole step
+        res = run(ic, tol=tol, steps=warmup + steps, sample=sample, threads=cores, sample_only=True)
+        rb = res["info"]["steps"][warmup:]
+        rebuild_steps = len(rb)
+        step_s = [x["t_domain"] + x["t_gravity"] for x in rb]
+        per_list = [max(x["t_gravity"] - x["t_build"], 1e-12) / ns for x in rb]
+    else:
+        rebuild_steps = max(1, int(rebuild_steps))
+        res = run(ic, tol=tol, steps=rebuild_steps + warmup + steps, sample=sample, threads=cores, sample_only=True,
+                  rebuild_steps=rebuild_steps)
+        st = res["info"]["steps"]
+        rb = st[:rebuild_steps]
+        timed = st[rebuild_steps + warmup:] or [dict(x, t_gravity=x["t_gravity"] - x["t_build"]) for x in rb]
+        step_s = [x["t_gravity"] for x in timed]
+        # a walk's time = a part paid once per call (loops over every
+        # particle, buffers; measured by a call with no target) + a time per
+        # target; the per-target part is what scales to n_eval
+        fixed = min(res["info"].get("empty_walk_s", 0.0), 0.9 * min(step_s))
+        per_list = [max(t - fixed, 1e-12) / ns for t in step_s]
+    t_domain = float(np.mean([x["t_domain"] for x in rb]))
+    t_build = float(np.mean([x["t_build"] for x in rb]))
+    rates = [n_eval / (t_domain + t_build + fixed + per * n_eval) for per in per_list]
     info = {"unit": "particles/s", "cores": cores, "kind": "reference",
-            "sample": "GIZMO's own domain_Decomposition + tree build + relative gravity walk (compiled reference, "
-                      "FP64, OpenMP %d threads) with %d seeded random active targets of %d; walk time per target "
-                      "scaled to the %d targets of a step" % (cores, ns, n, n_eval),
-            "t_domain_s": last["t_domain"], "t_build_s": last["t_build"],
-            "t_walk_per_particle_us": float(np.mean(per_list)) * 1e6}
+            "sample": "GIZMO's own domain_Decomposition + tree build (timed in %d rebuild step(s)) and relative "
+                      "gravity walk (compiled reference, FP64, OpenMP %d threads) of %s of %d, walked %d times on "
+                      "the resident tree; a step of %d targets is modelled as rebuild + the walk's fixed part + "
+                      "walk time per sampled target x %d" % (rebuild_steps, cores, sample_kind or "%d targets" % ns, n, len(step_s),
+                                       n_eval, n_eval),
+            "t_domain_s": t_domain, "t_build_s": t_build, "t_walk_fixed_s": fixed,
+            "t_empty_walk_s": res["info"].get("empty_walk_s"),
+            "t_walk_per_particle_us": float(np.mean(per_list)) * 1e6, "step_s": step_s, "sample_n": int(ns),
+            "startup": res["info"].get("startup"), "targets": sample, "acc": res["acc"][sample],
+            "pot": res["pot"][sample]}
     return rates, info
 
 
 def rate(ic, seconds=15.0, seed=1, tol=0.0025, threads=None, active_n=None):
     """One bounded measurement of the reference's step rate (about `seconds` of walk)."""
     n = ic["pos"].shape[0]
-    probe, pinfo = steps_rate(ic, steps=1, warmup=0, sample_n=512, seed=seed, tol=tol, threads=threads)
+    probe, pinfo = steps_rate(ic, steps=1, warmup=0, sample=512, seed=seed, tol=tol, threads=threads)
     per = pinfo["t_walk_per_particle_us"] * 1e-6
     ns = int(min(n, max(512, seconds / max(per, 1e-9))))
-    rates, info = steps_rate(ic, steps=1, warmup=0, sample_n=ns, seed=seed + 1, tol=tol, threads=threads,
+    rates, info = steps_rate(ic, steps=1, warmup=0, sample=ns, seed=seed + 1, tol=tol, threads=threads,
                              active_n=active_n)
     info["value"] = float(np.mean(rates))
     return info

@@ -221,8 +221,10 @@ def test_full_size_galaxy_properties():
     ic = ics.galaxy()
     n = ic["pos"].shape[0]
     with ggb200.GravityTree() as t:
-        acc, pot, nint, st = _two_pass(t, ic)
-        acc2, _, _, _ = t.evaluate(old_acc=None)   # re-walk with device-resident OldAcc
+        acc, pot, nint, st = _two_pass(t, ic, tol=0.001)
+        old = np.linalg.norm(acc, axis=1)
+        acc2, _, nint2, _ = t.evaluate(old_acc=old, err_tol_force_acc=0.001, want_ninter=True)
+        acc3, _, nint3, _ = t.evaluate(old_acc=old, err_tol_force_acc=0.001, want_ninter=True)
     assert st["error_word"] == 0
     tg = np.sort(np.random.default_rng(5).choice(n, 4096, replace=False)).astype(np.int32)
     dp, dm, dh = (torch.from_numpy(ic[k]).cuda() for k in ("pos", "mass", "h"))
@@ -230,7 +232,10 @@ def test_full_size_galaxy_properties():
     ggb200.direct_sum_fp64(dp, dm, dh, n, torch.from_numpy(tg).cuda(), tg.size, da, None)
     torch.cuda.synchronize()
     p50, p99, _ = ics.error_stats(acc[tg], da.cpu().numpy())
-    assert p99 < 5e-3, (p50, p99)
+    assert p99 < 2e-3, (p50, p99)   # the metric's bound, at the benchmark's tolerance
+    # two walks from the same OldAcc give the same bits (the second one runs its
+    # groups in another order, by the first one's measured costs)
+    assert np.array_equal(acc2, acc3) and np.array_equal(nint2, nint3)
     ptot = (ic["mass"][:, None] * acc).sum(0)
     assert np.linalg.norm(ptot) < 1e-3 * (ic["mass"][:, None] * np.abs(acc)).sum()
     assert st["interactions"] == nint.sum()
