@@ -207,6 +207,9 @@ def cpu_reference(ic, ref_tg, args, n_eval):
                              "t_walk_per_particle_us": i_rand["t_walk_per_particle_us"]},
            "random_over_ph_blocks": v_rand / v_ph, "host_cpu": host_cpu()}
     res = {"acc": i_rand["acc"], "pot": i_rand["pot"]}
+    if i_rand.get("startup") and ref_tg.size:
+        # the reference's own interactions per target (Costtotal of its relative pass over the sample)
+        res["interactions_per_target"] = float(i_rand["startup"]["cost_rel"]) / ref_tg.size
     return cpu, res
 
 
@@ -846,6 +849,19 @@ def run_system(args, torch, ggb200, dist, world, rank, local):
     tree.evaluate_device(d_acc, d_pot, err_tol_theta=0.7)
     tree.build()
     tree.evaluate_device(d_acc, d_pot, err_tol_force_acc=args.tol, err_tol_theta=0.0)
+    # the project's autotuner picks leaf and group size, flush threshold,
+    # blocks per SM and node staging on this system, refusing any candidate
+    # less accurate than the default configuration (outside the timed region)
+    tuned, tuned_ms, t_tune = None, None, 0.0
+    if not args.no_autotune:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        tuned, tuned_ms = tree.autotune(err_tol_force_acc=args.tol)
+        t_tune = time.perf_counter() - t0
+        kw.update(leaf_size=tuned["leaf_size"], group_size=tuned["group_size"], flush=tuned["flush"],
+                  blocks_per_sm=tuned["blocks_per_sm"], node_staging=tuned["node_staging"])
+        tree.build()
+        tree.evaluate_device(d_acc, d_pot, err_tol_force_acc=args.tol, err_tol_theta=0.0)
 
     act, d_act, na = None, None, n
     if args.active_frac < 1.0:
@@ -902,9 +918,25 @@ def run_system(args, torch, ggb200, dist, world, rank, local):
         d_sub = torch.from_numpy(sub).to(dev)
         d_acc_s = torch.empty((sub.size, 3), dtype=torch.float64, device=dev)
         d_pot_s = torch.empty(sub.size, dtype=torch.float64, device=dev)
-        walk_s = walker(tree, d_sub, int(sub.size), d_acc_s, d_pot_s)
+        # a context of its own, from the default configuration, tuned on the
+        # subset walk (sparser groups than the all-particle walk's); OldAcc of
+        # every particle from the all-particle walk
+        kw_s = dict(leaf_size=args.leaf, group_size=args.group, flush=args.flush, device=local,
+                    blocks_per_sm=args.blocks_per_sm, target_order=args.target_order, group_order=args.group_order,
+                    node_staging=args.node_staging)
+        tsub = ggb200.GravityTree(**kw_s)
+        tsub.set_stream(stream.cuda_stream)
+        tsub.load_device(d_rec, [n])
+        tsub.build()
+        old_all = torch.linalg.norm(d_acc, dim=1).contiguous() if act is None else None
+        tsub.evaluate_device(d_acc_s, d_pot_s, d_active=d_sub, n_active=int(sub.size), d_old_acc=old_all,
+                             err_tol_force_acc=args.tol, err_tol_theta=0.0)
+        tuned_s = None
+        if not args.no_autotune:
+            tuned_s, _ = tsub.autotune(err_tol_force_acc=args.tol, d_active=d_sub, n_active=int(sub.size))
+        walk_s = walker(tsub, d_sub, int(sub.size), d_acc_s, d_pot_s)
         for _ in range(args.warmup):
-            tree.build()
+            tsub.build()
             walk_s()
         torch.cuda.synchronize()
         if dist:
@@ -912,19 +944,21 @@ def run_system(args, torch, ggb200, dist, world, rank, local):
         clocks_s = ClockSampler(local)
         clocks_s.start()
         time.sleep(0.3)
-        tot_s, build_s, walk_s_ms = timed_steps(torch, stream, tree, walk_s, args.steps)
+        tot_s, build_s, walk_s_ms = timed_steps(torch, stream, tsub, walk_s, args.steps)
         clk_s = clocks_s.stop()
         tot_s = multi.max_over_ranks(dist, tot_s, device=dev)
         n_sub_all = multi.sum_over_ranks(dist, int(sub.size), device=dev)
-        st_s = tree.last_stats()
+        st_s = tsub.last_stats()
         if st_s["error_word"]:
             raise RuntimeError("device error word %d in the subset steps" % st_s["error_word"])
         subset = {"active": int(sub.size), "fraction": args.subset_frac, "value": n_sub_all / (tot_s / args.steps * 1e-3),
                   "unit": "targets/s", "ms_per_step": tot_s / args.steps, "build_ms": build_s, "walk_ms": walk_s_ms,
                   "interactions_per_target": st_s["interactions"] / sub.size, "clocks": clk_s,
                   "step": "full rebuild + relative walk of a seeded random %g of the particles" % args.subset_frac,
+                  "tuned": tuned_s,
                   "_targets": sub, "_acc": d_acc_s.cpu().numpy(), "_pot": d_pot_s.cpu().numpy()}
         del d_acc_s, d_pot_s
+        tsub.close()
 
     # stage breakdown on one extra instrumented step (outside the timed region)
     tprof = ggb200.GravityTree(timing=True, **kw)
@@ -1026,6 +1060,8 @@ def run_system(args, torch, ggb200, dist, world, rank, local):
                 subset["cpu_baseline"] = subset_reference_rate(cpu, subset["active"])
     if ref_cmp:
         force_error["vs_reference_tree"] = ref_cmp
+        if ref_res.get("interactions_per_target"):
+            ref_cmp["reference_interactions_per_target"] = ref_res["interactions_per_target"]
     if subset:
         sp50, sp99, _ = ics.error_stats(subset["_acc"][np.searchsorted(subset["_targets"], ref_tg)], acc_rdir)
         subset["force_error"] = sub_cmp or {"p50": sp50, "p99": sp99, "targets": int(ref_tg.size)}
@@ -1040,9 +1076,11 @@ def run_system(args, torch, ggb200, dist, world, rank, local):
                    "walk": "potential only (compute_potential)" if args.potential else "force and potential",
                    "step": "extent+keys+sort+permute+tree+moments+relative walk (OldAcc on device)",
                    "l2": "inputs larger than L2 (32 B/particle records, %d MB + tree)" % (32 * n // 10 ** 6),
-                   "leaf_size": args.leaf, "group_size": args.group, "flush": args.flush,
+                   "leaf_size": kw["leaf_size"], "group_size": kw["group_size"], "flush": kw["flush"],
+                   "blocks_per_sm": kw["blocks_per_sm"] or 2,
                    "group_order": "by previous walk's cost" if args.group_order else "target order",
-                   "node_staging": ["cp.async per lane", "bulk copies (TMA) per run"][args.node_staging],
+                   "node_staging": ["cp.async per lane", "bulk copies (TMA) per run"][kw["node_staging"]],
+                   "autotuned": tuned is not None, "autotune_walk_ms": tuned_ms, "autotune_s": t_tune,
                    "parallelism": "independent system per GPU" if world > 1 else "1 GPU"},
         "force_error": force_error,
         "interactions_per_step": inter, "interactions_per_s": inter / (ms_step * 1e-3),
@@ -1062,6 +1100,12 @@ def run_system(args, torch, ggb200, dist, world, rank, local):
                           "peak_source": hbm_src},
         "clocks": clk, "gpu_launches": int(launches), "e2e": e2e, "cpu_baseline": cpu,
     }
+    if ref_cmp and ref_cmp.get("reference_interactions_per_target") and out["roofline"]["frac"]:
+        # the same walk time credited with the reference tree's interaction
+        # count only: the FP32 fraction of useful work
+        ratio = ref_cmp["reference_interactions_per_target"] / (inter / na)
+        out["roofline"]["frac_at_reference_interactions"] = out["roofline"]["frac"] * ratio
+        out["roofline"]["interactions_vs_reference"] = 1.0 / ratio
     if subset:
         out["active_subset"] = subset
     if rank == 0:

@@ -216,6 +216,7 @@ struct gg_ctx {
     // drift of the resident tree (force_drift_node): velocities in load order,
     // node kinematics {vs, vmax} of the current build, per-system steps
     DevBuf<double> vel;
+    DevBuf<double> newpos;                // gg_set_positions: the caller's positions, load order
     bool have_vel = false;
     DevBuf<double4> kin;
     DevBuf<int> kin_counter;
@@ -241,8 +242,13 @@ struct gg_ctx {
     DevBuf<int> stack;
     DevBuf<int> err;
     DevBuf<double> acc_d, pot_d;
+    // autotuner accuracy gate: sampled targets, their FP64 direct sums and a
+    // configuration's outputs gathered at them
+    DevBuf<int2> tune_tg, tune_rows;
+    DevBuf<double> tune_acc, tune_pot, tune_mass, tune_gacc, tune_gpot;
     DevBuf<int> nint_d;
     int walk_blocks = 0;
+    int tune_tried = 0, tune_refused = 0;   // the last gg_autotune: trials, and trials the accuracy gate refused
     // host staging
     HostBuf<GGPart> h_stage;
     // timing
@@ -277,10 +283,11 @@ struct gg_ctx {
         f(keys); f(perm); f(rank); f(sort_scratch);
         f(t_start); f(t_end); f(t_level); f(t_parent); f(t_sys); f(t_nch); f(t_child); f(t_counter); f(t_bnd);
         f(t_depth); f(t_nnodes); f(t_bsum); f(t_boff); f(t_mass64); f(nodes);
-        f(oldacc); f(vel); f(kin); f(kin_counter); f(dts); f(oldacc_save); f(tcost); f(gkey); f(gorder);
+        f(oldacc); f(vel); f(newpos); f(kin); f(kin_counter); f(dts); f(oldacc_save); f(tcost); f(gkey); f(gorder);
         f(e_chunks); f(e_first); f(e_part); f(e_out);
         f(groups); f(ngroups); f(gscan); f(toff); f(flag); f(flagscan); f(tlist); f(tout); f(scan_scratch);
         f(active_d); f(counters); f(inter); f(stack); f(err); f(acc_d); f(pot_d); f(nint_d); f(oldacc_in);
+        f(tune_tg); f(tune_rows); f(tune_acc); f(tune_pot); f(tune_mass); f(tune_gacc); f(tune_gpot);
     }
 };
 
@@ -544,12 +551,13 @@ extern "C" gg_status gg_load_particles_device(gg_ctx *c, int32_t S, const int64_
 }
 
 // ---------------------------------------------------------------- build
-static int sys_passes(int S)
+// bits of a system id (0 for one system): the sort's last passes order by it
+static int sys_bits(int S)
 {
     if (S <= 1) return 0;
     int bits = 0;
     while ((1 << bits) < S) bits++;
-    return (bits + 7) / 8;
+    return bits;
 }
 
 static gg_status ensure_tree(gg_ctx *c)
@@ -585,8 +593,8 @@ extern "C" gg_status gg_build(gg_ctx *c, const gg_domain *domains)
     if ((st = set_device(c))) return st;
     cudaStream_t s = c->stream;
     const int S = c->S, N = (int)c->N;
-    int nsys = sys_passes(S), np = 8 + nsys;
-    if ((st = c->sort_scratch.ensure(gg_sort_scratch_bytes(N, np)))) return st;
+    const int sbits = sys_bits(S);
+    if ((st = c->sort_scratch.ensure(gg_sort_scratch_bytes(N)))) return st;
     if ((st = ensure_tree(c))) return st;
     GG_CUDA_TRY(cudaMemsetAsync(c->err.p, 0, 8 * sizeof(int), s));
     bool timing = c->cfg.timing != 0;
@@ -608,7 +616,8 @@ extern "C" gg_status gg_build(gg_ctx *c, const gg_domain *domains)
     if (N > 0) gg_launch_keys(c->in_rec.p, N, c->poff.p, S, c->dom.p, c->keys.p, c->perm.p, c->err.p, s);
     if (timing) cudaEventRecord(c->ev[1], s);
     if (N > 1) {
-        st = gg_sort_pairs_run(c->keys.p, c->perm.p, N, 8, nsys, c->poff.p, S, c->sort_scratch.p, c->err.p, s);
+        st = gg_sort_pairs_run(c->keys.p, c->perm.p, N, 3 * GG_MAX_LEVEL, sbits, c->poff.p, S, c->sort_scratch.p,
+                               c->err.p, s);
         if (st) return st;
     }
     if (timing) cudaEventRecord(c->ev[2], s);
@@ -653,7 +662,7 @@ static gg_status walk_setup(gg_ctx *c)
         return st;
     if (c->cfg.group_order &&
         ((st = c->tcost.ensure(c->N + 1)) || (st = c->gkey.ensure(maxg)) || (st = c->gorder.ensure(maxg)) ||
-         (st = c->sort_scratch.ensure(gg_sort_scratch_bytes(maxg, 1)))))
+         (st = c->sort_scratch.ensure(gg_sort_scratch_bytes(maxg)))))
         return st;
     return GG_OK;
 }
@@ -917,15 +926,14 @@ extern "C" gg_status gg_radix_sort_pairs(int64_t n, uint64_t *d_keys, uint32_t *
     if (n <= 1) return GG_OK;
     if (n >= (1ll << 30)) return GG_ERR_TOO_LARGE;
     cudaStream_t s = (cudaStream_t)stream;
-    int np = (key_bits + 7) / 8;
-    size_t bytes = gg_sort_scratch_bytes(n, np);
+    size_t bytes = gg_sort_scratch_bytes(n);
     void *scratch = nullptr;
     int *err = nullptr;
     GG_CUDA_TRY(cudaMallocAsync(&scratch, bytes, s));
     cudaError_t e = cudaMallocAsync((void **)&err, 64, s);
     if (e != cudaSuccess) { cudaFreeAsync(scratch, s); return gg_cuda_fail(e); }
     cudaMemsetAsync(err, 0, 64, s);
-    gg_status st = gg_sort_pairs_run((unsigned long long *)d_keys, d_vals, n, np, 0, nullptr, 1, scratch, err, s);
+    gg_status st = gg_sort_pairs_run((unsigned long long *)d_keys, d_vals, n, key_bits, 0, nullptr, 1, scratch, err, s);
     int herr = 0;
     cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s);
     cudaFreeAsync(scratch, s);
@@ -999,15 +1007,161 @@ extern "C" gg_status gg_graph_launch(gg_ctx *c)
 // other node staging on the winner.  Every trial
 // walks from the same OldAcc, so trials see the same opening decisions for a
 // given tree; the fastest configuration is kept and the tree rebuilt with it.
+// ---------------------------------------------------------------- autotuner accuracy gate
+// A faster configuration is only taken if it is no less accurate, per system,
+// than the configuration the context had (the default one, whose errors the
+// parity tests hold to the reference tree's).  Accuracy is measured on a fixed
+// sample of targets against their FP64 direct sums: every target of a system
+// of up to 2,048 particles, else 16,384 / S targets (at least 64, at most
+// 4,096) evenly spaced in load order, S being the number of systems.  A
+// candidate passes when, for every system, its 99th-percentile relative force
+// error is at most 1.1x the base configuration's (plus 1e-7 for systems whose
+// error is at rounding level) and its sample potential energy W = 1/2 sum m phi
+// is no further from the direct sum's than 1.1x the base configuration's, or
+// within 1e-5 of it.
+static const int kTuneAllBelow = 2048, kTuneBudget = 16384, kTuneMin = 64, kTuneMax = 4096;
+
+struct TuneRef {
+    std::vector<int2> tg;                 // (load index, system) of each sampled target
+    std::vector<int2> rows;               // (output row, 0) of each sampled target
+    std::vector<int> first;               // first sample row of each system (S + 1 entries)
+    std::vector<double> acc_dir, pot_dir, mass;
+};
+struct TuneErr {
+    std::vector<double> p99, werr, wdir;  // per system
+};
+
+// The sample: in each system, its targets (all of them, or the walk's active
+// ones), every one of them up to kTuneAllBelow, else `per` evenly spaced in
+// walk order.  h_active: the active load indices (n_active), or null for all.
+static gg_status tune_reference(gg_ctx *c, TuneRef &R, const int *h_active, long long n_active)
+{
+    gg_status st;
+    R.tg.clear();
+    R.rows.clear();
+    R.first.assign(c->S + 1, 0);
+    const long long per = std::min<long long>(kTuneMax, std::max<long long>(kTuneMin, kTuneBudget / c->S));
+    std::vector<std::vector<int>> act_rows;   // per system, the rows of its active targets
+    if (h_active) {
+        act_rows.resize(c->S);
+        for (long long r = 0; r < n_active; r++) {
+            const int i = h_active[r];
+            if (i < 0 || i >= c->N) return GG_ERR_INVALID;
+            const int s = (int)(std::upper_bound(c->h_poff.begin(), c->h_poff.begin() + c->S + 1, i) -
+                                c->h_poff.begin()) - 1;
+            act_rows[s].push_back((int)r);
+        }
+    }
+    for (int s = 0; s < c->S; s++) {
+        const long long o = c->h_poff[s];
+        const long long n = h_active ? (long long)act_rows[s].size() : c->h_poff[s + 1] - o;
+        R.first[s] = (int)R.tg.size();
+        const long long k = n <= kTuneAllBelow ? n : per;
+        for (long long j = 0; j < k; j++) {
+            const long long q = n <= kTuneAllBelow ? j : (2 * j + 1) * n / (2 * k);   // q-th target of the system
+            const int row = h_active ? act_rows[s][q] : (int)(o + q);
+            R.tg.push_back(make_int2(h_active ? h_active[row] : row, s));
+            R.rows.push_back(make_int2(row, 0));
+        }
+    }
+    R.first[c->S] = (int)R.tg.size();
+    const int nt = (int)R.tg.size();
+    if ((st = c->tune_tg.ensure(nt)) || (st = c->tune_rows.ensure(nt)) || (st = c->tune_acc.ensure(3 * (size_t)nt)) ||
+        (st = c->tune_pot.ensure(nt)) || (st = c->tune_mass.ensure(nt)) || (st = c->tune_gacc.ensure(3 * (size_t)nt)) ||
+        (st = c->tune_gpot.ensure(nt)))
+        return st;
+    GG_CUDA_TRY(cudaMemcpyAsync(c->tune_tg.p, R.tg.data(), nt * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
+    GG_CUDA_TRY(cudaMemcpyAsync(c->tune_rows.p, R.rows.data(), nt * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
+    gg_launch_direct_records(c->in_rec.p, c->poff.p, c->tune_tg.p, nt, c->tune_acc.p, c->tune_pot.p, c->tune_mass.p,
+                             c->stream);
+    R.acc_dir.resize(3 * (size_t)nt);
+    R.pot_dir.resize(nt);
+    R.mass.resize(nt);
+    GG_CUDA_TRY(cudaMemcpyAsync(R.acc_dir.data(), c->tune_acc.p, 3 * nt * sizeof(double), cudaMemcpyDeviceToHost,
+                                c->stream));
+    GG_CUDA_TRY(cudaMemcpyAsync(R.pot_dir.data(), c->tune_pot.p, nt * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    GG_CUDA_TRY(cudaMemcpyAsync(R.mass.data(), c->tune_mass.p, nt * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    GG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    GG_CUDA_TRY(cudaGetLastError());
+    return GG_OK;
+}
+
+// p-th percentile with linear interpolation between order statistics
+static double percentile(std::vector<double> v, double q)
+{
+    if (v.empty()) return 0.0;
+    std::sort(v.begin(), v.end());
+    const double x = q / 100.0 * (double)(v.size() - 1);
+    const size_t i = (size_t)x;
+    return i + 1 < v.size() ? v[i] + (x - (double)i) * (v[i + 1] - v[i]) : v[i];
+}
+
+// errors of the outputs the last walk left in acc_d / pot_d (load order)
+static gg_status tune_errors(gg_ctx *c, const TuneRef &R, TuneErr &E)
+{
+    const int nt = (int)R.tg.size();
+    gg_launch_gather_rows(c->acc_d.p, c->pot_d.p, c->tune_rows.p, nt, c->tune_gacc.p, c->tune_gpot.p, c->stream);
+    std::vector<double> a(3 * (size_t)nt), p(nt);
+    GG_CUDA_TRY(cudaMemcpyAsync(a.data(), c->tune_gacc.p, 3 * nt * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    GG_CUDA_TRY(cudaMemcpyAsync(p.data(), c->tune_gpot.p, nt * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    GG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    E.p99.assign(c->S, 0.0);
+    E.werr.assign(c->S, 0.0);
+    E.wdir.assign(c->S, 0.0);
+    for (int s = 0; s < c->S; s++) {
+        std::vector<double> e;
+        double w = 0, wd = 0;
+        for (int t = R.first[s]; t < R.first[s + 1]; t++) {
+            double d2 = 0, r2 = 0;
+            for (int k = 0; k < 3; k++) {
+                const double d = a[3 * (size_t)t + k] - R.acc_dir[3 * (size_t)t + k];
+                d2 += d * d;
+                r2 += R.acc_dir[3 * (size_t)t + k] * R.acc_dir[3 * (size_t)t + k];
+            }
+            if (r2 > 0) e.push_back(sqrt(d2 / r2));
+            w += 0.5 * R.mass[t] * p[t];
+            wd += 0.5 * R.mass[t] * R.pot_dir[t];
+        }
+        E.p99[s] = percentile(e, 99.0);
+        E.werr[s] = fabs(w - wd);
+        E.wdir[s] = fabs(wd);
+    }
+    return GG_OK;
+}
+
+static bool tune_accepts(const TuneErr &base, const TuneErr &cand)
+{
+    for (size_t s = 0; s < base.p99.size(); s++) {
+        if (!(cand.p99[s] <= 1.1 * base.p99[s] + 1e-7)) return false;
+        if (!(cand.werr[s] <= std::max(1.1 * base.werr[s], 1e-5 * base.wdir[s]))) return false;
+    }
+    return true;
+}
+
 extern "C" gg_status gg_autotune(gg_ctx *c, double tol, double theta, gg_config *chosen, double *best_ms)
 {
-    if (!c || tol < 0 || theta < 0) return GG_ERR_INVALID;
+    return gg_autotune_active(c, nullptr, 0, tol, theta, chosen, best_ms);
+}
+
+extern "C" gg_status gg_autotune_active(gg_ctx *c, const int32_t *d_active, int64_t n_active, double tol, double theta,
+                                        gg_config *chosen, double *best_ms)
+{
+    if (!c || tol < 0 || theta < 0 || n_active < 0 || (n_active && !d_active)) return GG_ERR_INVALID;
     if (!c->built) return GG_ERR_NOT_BUILT;
+    if (n_active > c->N) return GG_ERR_INVALID;
     gg_status st;
     if ((st = set_device(c))) return st;
     cudaStream_t s = c->stream;
     const long long N = c->N;
-    if ((st = c->acc_d.ensure(N * 3 + 3))) return st;
+    if ((st = c->acc_d.ensure(N * 3 + 3)) || (st = c->pot_d.ensure(N + 1))) return st;
+    if (!n_active) d_active = nullptr;
+    std::vector<int> h_active(d_active ? n_active : 0);
+    if (d_active) {
+        GG_CUDA_TRY(cudaMemcpyAsync(h_active.data(), d_active, n_active * sizeof(int), cudaMemcpyDeviceToHost, s));
+        GG_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    TuneRef R;
+    if ((st = tune_reference(c, R, d_active ? h_active.data() : nullptr, n_active))) return st;
     const bool had_old = c->oldacc_valid;
     if (had_old && ((st = c->oldacc_save.ensure(N + 1)))) return st;
     if (had_old)
@@ -1022,8 +1176,12 @@ extern "C" gg_status gg_autotune(gg_ctx *c, double tol, double theta, gg_config 
     gg_config best_cfg = base;
     int best_blocks = base_blocks;
     st = GG_OK;
-    // one configuration: the faster of two timed walks from the same OldAcc
-    auto trial = [&](float *ms_out) -> gg_status {
+    TuneErr base_err, err;
+    int tried = 0, refused = 0;
+    // one configuration: the faster of two timed walks from the same OldAcc,
+    // and whether its outputs pass the accuracy gate against the base
+    // configuration's (the first call measures the base itself)
+    auto trial = [&](float *ms_out, bool *ok) -> gg_status {
         float ms_min = 1e30f;
         for (int rep = 0; rep < 2; rep++) {
             if (had_old) {
@@ -1033,7 +1191,7 @@ extern "C" gg_status gg_autotune(gg_ctx *c, double tol, double theta, gg_config 
             }
             c->oldacc_valid = had_old;
             cudaEventRecord(e0, s);
-            gg_status r = run_walk(c, nullptr, 0, nullptr, tol, theta, c->acc_d.p, nullptr, nullptr);
+            gg_status r = run_walk(c, d_active, (int)n_active, nullptr, tol, theta, c->acc_d.p, c->pot_d.p, nullptr);
             cudaEventRecord(e1, s);
             if (r) return r;
             if ((r = collect_stats(c, nullptr))) return r;
@@ -1042,8 +1200,21 @@ extern "C" gg_status gg_autotune(gg_ctx *c, double tol, double theta, gg_config 
             if (ms < ms_min) ms_min = ms;
         }
         *ms_out = ms_min;
+        gg_status r = tune_errors(c, R, err);
+        if (r) return r;
+        if (base_err.p99.empty()) base_err = err;
+        *ok = tune_accepts(base_err, err);
+        tried++;
+        if (!*ok) refused++;
         return GG_OK;
     };
+    // the base configuration first: its errors are the gate's bar
+    {
+        float ms = 0;
+        bool ok = false;
+        st = trial(&ms, &ok);
+        if (!st) best = ms;
+    }
     for (int li = 0; li < 2 && !st; li++) {
         c->cfg.leaf_size = leafs[li];
         if ((st = gg_build(c, nullptr))) break;
@@ -1054,8 +1225,9 @@ extern "C" gg_status gg_autotune(gg_ctx *c, double tol, double theta, gg_config 
                     c->cfg.flush_threshold = flushes[fi];
                     c->walk_blocks = bpss[bi];
                     float ms = 0;
-                    if ((st = trial(&ms))) break;
-                    if (ms < best) {
+                    bool ok = false;
+                    if ((st = trial(&ms, &ok))) break;
+                    if (ok && ms < best) {
                         best = ms;
                         best_cfg = c->cfg;
                         best_blocks = c->walk_blocks;
@@ -1068,7 +1240,8 @@ extern "C" gg_status gg_autotune(gg_ctx *c, double tol, double theta, gg_config 
         c->walk_blocks = best_blocks;
         c->cfg.node_staging = 1 - best_cfg.node_staging;
         float ms = 0;
-        if (!(st = gg_build(c, nullptr)) && !(st = trial(&ms)) && ms < best) {
+        bool ok = false;
+        if (!(st = gg_build(c, nullptr)) && !(st = trial(&ms, &ok)) && ok && ms < best) {
             best = ms;
             best_cfg = c->cfg;
         }
@@ -1088,7 +1261,64 @@ extern "C" gg_status gg_autotune(gg_ctx *c, double tol, double theta, gg_config 
     if (!st) st = st2;
     if (!st && chosen) *chosen = c->cfg;
     if (!st && best_ms) *best_ms = best;
+    c->tune_tried = tried;
+    c->tune_refused = refused;
     return st;
+}
+
+// The accuracy gate of gg_autotune for one candidate configuration against
+// the context's own, from the same OldAcc; the context is left as it was.
+extern "C" gg_status gg_tune_accuracy(gg_ctx *c, double tol, double theta, const gg_config *cand, int32_t *accepted)
+{
+    if (!c || !cand || !accepted || tol < 0 || theta < 0) return GG_ERR_INVALID;
+    if (cand->leaf_size < 1 || cand->leaf_size > 32 || cand->group_size < 1 || cand->group_size > 64 ||
+        cand->flush_threshold < 32 || cand->flush_threshold > 128 || cand->walk_blocks_per_sm < 0 ||
+        cand->walk_blocks_per_sm > 3 || cand->node_staging < 0 || cand->node_staging > 1)
+        return GG_ERR_INVALID;
+    if (!c->built) return GG_ERR_NOT_BUILT;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    cudaStream_t s = c->stream;
+    const long long N = c->N;
+    if ((st = c->acc_d.ensure(N * 3 + 3)) || (st = c->pot_d.ensure(N + 1))) return st;
+    TuneRef R;
+    if ((st = tune_reference(c, R, nullptr, 0))) return st;
+    const bool had_old = c->oldacc_valid;
+    if (had_old && ((st = c->oldacc_save.ensure(N + 1)))) return st;
+    if (had_old)
+        GG_CUDA_TRY(cudaMemcpyAsync(c->oldacc_save.p, c->oldacc.p, N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    auto walk_errors = [&](TuneErr &E) -> gg_status {
+        if (had_old)
+            GG_CUDA_TRY(cudaMemcpyAsync(c->oldacc.p, c->oldacc_save.p, N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        c->oldacc_valid = had_old;
+        gg_status r = run_walk(c, nullptr, 0, nullptr, tol, theta, c->acc_d.p, c->pot_d.p, nullptr);
+        if (r || (r = collect_stats(c, nullptr))) return r;
+        return tune_errors(c, R, E);
+    };
+    TuneErr base, cerr;
+    if ((st = walk_errors(base))) return st;
+    const gg_config keep = c->cfg;
+    const int keep_blocks = c->walk_blocks;
+    c->cfg.leaf_size = cand->leaf_size;
+    c->cfg.group_size = cand->group_size;
+    c->cfg.flush_threshold = cand->flush_threshold;
+    c->cfg.node_staging = cand->node_staging;
+    c->cfg.target_order = cand->target_order;
+    c->cfg.group_order = cand->group_order;
+    if (cand->walk_blocks_per_sm > 0) c->walk_blocks = cand->walk_blocks_per_sm;
+    const bool rebuild = cand->leaf_size != keep.leaf_size;
+    if (rebuild) st = gg_build(c, nullptr);
+    if (!st) st = walk_errors(cerr);
+    if (!st) *accepted = tune_accepts(base, cerr) ? 1 : 0;
+    c->cfg = keep;
+    c->walk_blocks = keep_blocks;
+    gg_status st2 = rebuild ? gg_build(c, nullptr) : GG_OK;
+    if (had_old) {
+        cudaError_t ce = cudaMemcpyAsync(c->oldacc.p, c->oldacc_save.p, N * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        if (ce != cudaSuccess && !st2) st2 = gg_cuda_fail(ce);
+    }
+    c->oldacc_valid = had_old;
+    return st ? st : st2;
 }
 
 // ---------------------------------------------------------------- drift
@@ -1130,6 +1360,34 @@ extern "C" gg_status gg_load_velocities_device(gg_ctx *c, const double *d_vel)
                                     c->stream));
     c->have_vel = true;
     c->kin_valid = false;
+    return GG_OK;
+}
+
+extern "C" gg_status gg_set_positions(gg_ctx *c, const double *pos, int64_t pos_stride)
+{
+    if (!c || !pos || c->S < 1) return GG_ERR_INVALID;
+    if (!c->built) return GG_ERR_NOT_BUILT;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    if (pos_stride <= 0) pos_stride = 3 * sizeof(double);
+    const long long N = c->N;
+    if ((st = c->newpos.ensure((size_t)3 * N + 3))) return st;
+    if ((st = c->h_vstage.ensure((size_t)N * 3, c->vstage_ev))) return st;
+    const char *pb = (const char *)pos;
+    double *dst = c->h_vstage.p;
+    for (long long b = 0; b < N; b += kPipeChunk) {   // gather one chunk while the previous one is copied
+        const long long e = std::min(N, b + kPipeChunk);
+#pragma omp parallel for schedule(static)
+        for (long long i = b; i < e; i++) {
+            const double *x = (const double *)(pb + i * pos_stride);
+            dst[3 * i] = x[0]; dst[3 * i + 1] = x[1]; dst[3 * i + 2] = x[2];
+        }
+        GG_CUDA_TRY(cudaMemcpyAsync(c->newpos.p + 3 * b, dst + 3 * b, (size_t)(e - b) * 3 * sizeof(double),
+                                    cudaMemcpyHostToDevice, c->stream));
+    }
+    GG_CUDA_TRY(cudaEventRecord(c->vstage_ev, c->stream));
+    gg_launch_set_positions(c->in_rec.p, c->part.p, c->perm.p, c->newpos.p, (int)N, c->err.p, c->stream);
+    GG_CUDA_TRY(cudaGetLastError());
     return GG_OK;
 }
 
@@ -1472,6 +1730,18 @@ extern "C" gg_status gg_get_order(gg_ctx *c, int32_t *order_out)
     // perm holds the load index of each sorted position (uint32 < 2^30)
     GG_CUDA_TRY(cudaMemcpyAsync(order_out, c->perm.p, (size_t)c->N * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
     GG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return GG_OK;
+}
+
+extern "C" gg_status gg_get_order_device(gg_ctx *c, int32_t *d_order_out)
+{
+    if (!c || !d_order_out) return GG_ERR_INVALID;
+    if (!c->built) return GG_ERR_NOT_BUILT;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    if (c->N == 0) return GG_OK;
+    GG_CUDA_TRY(cudaMemcpyAsync(d_order_out, c->perm.p, (size_t)c->N * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                                c->stream));
     return GG_OK;
 }
 

@@ -112,6 +112,27 @@ __global__ void k_drift_particles(GGPart *__restrict__ in_rec, GGPart *__restric
     }
 }
 
+// The caller's current positions (load order, FP64 xyz) into the load-order
+// records and the sorted copy the walk reads; the tree is kept.  A non-finite
+// position is refused (error bit) and leaves that particle where it was.
+__global__ void k_set_positions(GGPart *__restrict__ in_rec, GGPart *__restrict__ parts,
+                                const unsigned *__restrict__ perm, const double *__restrict__ pos, int n,
+                                int *__restrict__ err)
+{
+    bool bad = false;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned j = perm[i];
+        if (j >= (unsigned)n) continue;   // only after a failed sort, which is reported
+        const double x = pos[3 * (size_t)j], y = pos[3 * (size_t)j + 1], z = pos[3 * (size_t)j + 2];
+        if (!isfinite(x) || !isfinite(y) || !isfinite(z)) { bad = true; continue; }
+        GGPart p = in_rec[j];
+        p.x = x; p.y = y; p.z = z;
+        in_rec[j] = p;
+        parts[i] = p;
+    }
+    if (bad) atomicOr(err, GG_EBIT_BAD_INPUT);
+}
+
 // s += vs*dt, len += 2*vmax*dt, geometric centre fixed (force_drift_node)
 __global__ void k_drift_nodes(GGNode *__restrict__ nodes, const double4 *__restrict__ kin, const int *__restrict__ sys,
                               const int *__restrict__ nnodes, const double *__restrict__ dts, double dt_all)
@@ -157,5 +178,13 @@ void gg_launch_drift(GGPart *in_rec, GGPart *parts, const unsigned *perm, const 
         gg_note_launches(1);
     }
     k_drift_nodes<<<grid_for(ncap, 256), 256, 0, st>>>(nodes, kin, node_sys, nnodes, dts, dt_all);
+    gg_note_launches(1);
+}
+
+void gg_launch_set_positions(GGPart *in_rec, GGPart *parts, const unsigned *perm, const double *pos, int n, int *err,
+                             cudaStream_t st)
+{
+    if (n < 1) return;
+    k_set_positions<<<grid_for(n, 256), 256, 0, st>>>(in_rec, parts, perm, pos, n, err);
     gg_note_launches(1);
 }

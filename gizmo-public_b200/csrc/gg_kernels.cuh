@@ -22,8 +22,9 @@ void gg_launch_keys(const GGPart *rec, int n, const int *poff, int S, const GGDo
 void gg_launch_keys_plain(const double *pos, long long n, const GGDomainDev &d, unsigned long long *keys, int *err,
                           cudaStream_t st);
 
-size_t gg_sort_scratch_bytes(long long n, int npasses);
-gg_status gg_sort_pairs_run(unsigned long long *keys, unsigned *vals, long long n, int nkey, int nsys,
+size_t gg_sort_scratch_bytes(long long n);
+int gg_sort_bits();
+gg_status gg_sort_pairs_run(unsigned long long *keys, unsigned *vals, long long n, int key_bits, int sys_bits,
                             const int *poff, int S, void *scratch, int *err, cudaStream_t st);
 
 void gg_launch_permute(const unsigned *perm, const GGPart *in, GGPart *out, unsigned *rank, int n, cudaStream_t st);
@@ -82,12 +83,18 @@ gg_status gg_order_targets_by_softening(int nt, const int *tlist_in, const int *
                                         unsigned *val, int *tlist_out, int *tout_out, void *sort_scratch, int *err,
                                         cudaStream_t st);
 
+void gg_launch_direct_records(const GGPart *rec, const int *poff, const int2 *tg, int ntg, double *acc, double *pot,
+                              double *mass, cudaStream_t st);
+void gg_launch_gather_rows(const double *acc, const double *pot, const int2 *tg, int ntg, double *acc_out,
+                           double *pot_out, cudaStream_t st);
 void gg_launch_direct(long long n_src, const double *pos, const double *mass, const double *h, long long n_tgt,
                       const int *targets, double *acc, double *pot, cudaStream_t st);
 
 // drift of a resident tree (gg_drift.cu)
 void gg_launch_node_kinematics(const GGPart *parts, const unsigned *perm, const double *vel, TreeBuf tb, int *counter,
                                double4 *kin, int n, int ncap, int keep_max, cudaStream_t st);
+void gg_launch_set_positions(GGPart *in_rec, GGPart *parts, const unsigned *perm, const double *pos, int n, int *err,
+                             cudaStream_t st);
 void gg_launch_drift(GGPart *in_rec, GGPart *parts, const unsigned *perm, const double *vel, const int *poff, int S,
                      const double *dts, double dt_all, GGNode *nodes, const double4 *kin, const int *node_sys, const int *nnodes,
                      int n, int ncap, cudaStream_t st);

@@ -20,8 +20,9 @@
 #include "gg_internal.cuh"
 #include "gg_kernels.cuh"
 
-// scratch of gg_sort_pairs_run for GG_NOALLOC_SORT_MAX_N pairs and 8 passes
-// (≈16.0 MB with 2048-key tiles), plus the error word in the last 256 bytes
+// scratch of gg_sort_pairs_run for GG_NOALLOC_SORT_MAX_N pairs (12.6 MB for
+// the alternate keys and values, 1 MB of look-back status words with 4096-key
+// tiles and 9-bit digits), plus the error word in the last 256 bytes
 #define GG_NOALLOC_SCRATCH_BYTES (20u << 20)
 
 static __device__ __align__(256) unsigned char gg_noalloc_scratch[GG_NOALLOC_SCRATCH_BYTES];
@@ -31,7 +32,10 @@ static void *g_noalloc_ptr[64];
 
 // Device address of the array on the current device.  In host code the
 // symbol name is only a host-side stand-in; the address is looked up once per
-// device, with that device current, on the first call there.
+// device, with that device current, on the first call there, and kept for the
+// life of the process.  A cudaDeviceReset by the application ends the
+// context the address belongs to: after one, this entry point must not be
+// called again in the same process.
 static gg_status noalloc_scratch(void **out)
 {
     int dev = 0;
@@ -54,15 +58,26 @@ extern "C" gg_status gg_radix_sort_pairs_noalloc(int64_t n, uint64_t *d_keys, ui
     if (n < 0 || key_bits < 1 || key_bits > 64 || (n && (!d_keys || !d_vals))) return GG_ERR_INVALID;
     if (n > GG_NOALLOC_SORT_MAX_N) return GG_ERR_TOO_LARGE;
     if (n <= 1) return GG_OK;
-    const int np = (key_bits + 7) / 8;
-    if (gg_sort_scratch_bytes(n, np) + 256 > GG_NOALLOC_SCRATCH_BYTES) return GG_ERR_TOO_LARGE;
+    if (gg_sort_scratch_bytes(n) + 256 > GG_NOALLOC_SCRATCH_BYTES) return GG_ERR_TOO_LARGE;
+    // the pairs must be device memory of the current device, where the array is
+    int dev = 0;
+    GG_CUDA_TRY(cudaGetDevice(&dev));
+    for (const void *ptr : {(const void *)d_keys, (const void *)d_vals}) {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+            cudaGetLastError();
+            return GG_ERR_INVALID;
+        }
+        if ((a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) || a.device != dev)
+            return GG_ERR_INVALID;
+    }
     void *scratch = nullptr;
     gg_status st = noalloc_scratch(&scratch);
     if (st) return st;
     cudaStream_t s = (cudaStream_t)stream;
     int *err = (int *)((char *)scratch + GG_NOALLOC_SCRATCH_BYTES - 256);
     GG_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), s));
-    st = gg_sort_pairs_run((unsigned long long *)d_keys, d_vals, n, np, 0, nullptr, 1, scratch, err, s);
+    st = gg_sort_pairs_run((unsigned long long *)d_keys, d_vals, n, key_bits, 0, nullptr, 1, scratch, err, s);
     if (st) return st;
     int herr = 0;
     GG_CUDA_TRY(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -3,13 +3,19 @@
 // Replaces the reference's stable mergesort of {peanokey, index} records
 // (mysort_peano, system/peano.c:414-462; mysort_domain, domain.c:2674-2723).
 // Design (one-sweep): one up-front pass builds the digit histograms of every
-// pass; each pass is then a single kernel in which a CTA ranks a 2048-key tile
-// in shared memory, publishes its per-digit counts, sums its predecessors'
-// counts with a decoupled look-back, and writes the tile out digit-sorted so
-// that global stores are contiguous runs.  8-bit digits.  For several systems
-// a second set of passes sorts stably by system id (taken from the value, an
+// pass; each pass is then a single kernel in which a CTA ranks a tile of
+// SORT_TILE keys in shared memory, publishes its per-digit counts, sums its
+// predecessors' counts with a decoupled look-back, and writes the tile out
+// digit-sorted so that global stores are contiguous runs.  SORT_BITS-bit
+// digits (9: the 63-bit Peano-Hilbert keys take 7 passes).  For several
+// systems further passes sort stably by system id (taken from the value, an
 // index into the concatenated particle array), so the final order is
 // (system, key).
+//
+// The look-back status words of a pass live in one of two arrays: pass p
+// reads and writes array p % 2 and clears its own tile's words of the other
+// array for pass p + 1 (whose tiles only start once every tile of pass p has
+// finished), so one memset before the first pass serves every pass.
 //
 // Every wait in the look-back is bounded: after GG_SORT_SPIN_LIMIT polls the
 // CTA records GG_EBIT_SORT_TIMEOUT in the error word and carries on, so a
@@ -17,16 +23,29 @@
 #include "gg_internal.cuh"
 #include "gg_kernels.cuh"
 
+#ifndef GG_SORT_BITS
+#define GG_SORT_BITS 9
+#endif
+#ifndef GG_SORT_ITEMS
+#define GG_SORT_ITEMS 16
+#endif
 #define SORT_THREADS 256
-#define SORT_ITEMS 8      // 2048-key tiles: 4 blocks of 8 warps fit an SM (registers and shared memory)
+#define SORT_ITEMS GG_SORT_ITEMS
 #define SORT_TILE (SORT_THREADS * SORT_ITEMS)
 #define SORT_WARPS (SORT_THREADS / 32)
-#define RADIX 256
+#define SORT_BITS GG_SORT_BITS
+#define RADIX (1 << SORT_BITS)
+#define DPT (RADIX / SORT_THREADS)          // digits per thread in the per-digit phases
 #define ST_AGG (1u << 30)
 #define ST_INC (2u << 30)
 #define ST_FLAGS (3u << 30)
 #define ST_VALUE 0x3FFFFFFFu
 #define GG_SORT_SPIN_LIMIT (1 << 22)
+
+static_assert(RADIX >= SORT_THREADS && RADIX % SORT_THREADS == 0, "each thread owns whole digits");
+static_assert(SORT_BITS * GG_SORT_MAX_PASSES >= 64 + 32, "enough passes for a 64-bit key and a system id");
+
+int gg_sort_bits() { return SORT_BITS; }
 
 __device__ __forceinline__ int sort_sys_of(const int *__restrict__ poff, int S, unsigned v)
 {
@@ -43,16 +62,17 @@ __device__ __forceinline__ int sort_sys_of(const int *__restrict__ poff, int S, 
 __global__ void k_sort_hist(const unsigned long long *__restrict__ keys, const unsigned *__restrict__ vals, int n,
                             int nkey, int nsys, const int *__restrict__ poff, int S, unsigned *g_hist)
 {
-    __shared__ unsigned sh[GG_SORT_MAX_PASSES * RADIX];
-    int np = nkey + nsys;
+    extern __shared__ unsigned sh[];   // (nkey + nsys) * RADIX
+    const int np = nkey + nsys;
     for (int i = threadIdx.x; i < np * RADIX; i += blockDim.x) sh[i] = 0;
     __syncthreads();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        unsigned long long k = keys[i];
-        for (int p = 0; p < nkey; p++) atomicAdd(&sh[p * RADIX + ((k >> (8 * p)) & 255)], 1u);
+        const unsigned long long k = keys[i];
+        for (int p = 0; p < nkey; p++) atomicAdd(&sh[p * RADIX + ((k >> (SORT_BITS * p)) & (RADIX - 1))], 1u);
         if (nsys) {
-            unsigned s = (unsigned)sort_sys_of(poff, S, vals[i]);
-            for (int p = 0; p < nsys; p++) atomicAdd(&sh[(nkey + p) * RADIX + ((s >> (8 * p)) & 255)], 1u);
+            const unsigned s = (unsigned)sort_sys_of(poff, S, vals[i]);
+            for (int p = 0; p < nsys; p++)
+                atomicAdd(&sh[(nkey + p) * RADIX + ((s >> (SORT_BITS * p)) & (RADIX - 1))], 1u);
         }
     }
     __syncthreads();
@@ -60,28 +80,41 @@ __global__ void k_sort_hist(const unsigned long long *__restrict__ keys, const u
         if (sh[i]) atomicAdd(&g_hist[i], sh[i]);
 }
 
-// exclusive scan of each pass's 256 counts (one block per pass, 256 threads)
-__global__ void k_sort_hist_scan(const unsigned *g_hist, unsigned *g_off)
+// block-wide exclusive scan of DPT consecutive values per thread (digits
+// DPT*tid .. DPT*tid+DPT-1); returns the thread's exclusive base and writes
+// each digit's exclusive prefix into excl[]
+__device__ __forceinline__ void block_excl_scan(const unsigned (&v)[DPT], unsigned (&excl)[DPT], unsigned *s_wsum)
 {
-    __shared__ unsigned ws[8];
-    int p = blockIdx.x, d = threadIdx.x, lane = d & 31, w = d >> 5;
-    unsigned v = g_hist[p * RADIX + d], x = v;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    unsigned t = 0;
+#pragma unroll
+    for (int q = 0; q < DPT; q++) { excl[q] = t; t += v[q]; }
+    unsigned x = t;
+#pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
         if (lane >= o) x += y;
     }
-    if (lane == 31) ws[w] = x;
+    if (lane == 31) s_wsum[w] = x;
     __syncthreads();
-    if (w == 0) {
-        unsigned t = lane < 8 ? ws[lane] : 0, u = t;
-        for (int o = 1; o < 8; o <<= 1) {
-            unsigned y = __shfl_up_sync(0xffffffffu, u, o);
-            if (lane >= o) u += y;
-        }
-        if (lane < 8) ws[lane] = u - t;
-    }
-    __syncthreads();
-    g_off[p * RADIX + d] = x - v + ws[w];
+    unsigned wo = 0;
+    for (int ww = 0; ww < w; ww++) wo += s_wsum[ww];
+    const unsigned base = x - t + wo;
+#pragma unroll
+    for (int q = 0; q < DPT; q++) excl[q] += base;
+}
+
+// exclusive scan of each pass's RADIX counts (one block of SORT_THREADS per pass)
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_hist_scan(const unsigned *g_hist, unsigned *g_off)
+{
+    __shared__ unsigned s_wsum[SORT_WARPS];
+    const int p = blockIdx.x;
+    unsigned v[DPT], e[DPT];
+#pragma unroll
+    for (int q = 0; q < DPT; q++) v[q] = g_hist[p * RADIX + DPT * threadIdx.x + q];
+    block_excl_scan(v, e, s_wsum);
+#pragma unroll
+    for (int q = 0; q < DPT; q++) g_off[p * RADIX + DPT * threadIdx.x + q] = e[q];
 }
 
 __device__ __forceinline__ unsigned ld_status(const unsigned *p)
@@ -95,26 +128,33 @@ __device__ __forceinline__ void st_status(unsigned *p, unsigned v)
     asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// one pass: digit = (key >> shift) & 255, or (system id >> shift) & 255 when sys_mode
-__global__ void __launch_bounds__(SORT_THREADS, 4) k_sort_pass(
+struct SortSmem {
+    unsigned long long keys[SORT_TILE];
+    unsigned vals[SORT_TILE];
+    unsigned short dig[SORT_TILE];
+    unsigned whist[SORT_WARPS][RADIX];
+    unsigned texcl[RADIX];
+    unsigned gbase[RADIX];
+    unsigned wsum[SORT_WARPS];
+    int tile;
+};
+
+// one pass: digit = (key >> shift) & (RADIX-1), or of the system id when sys_mode.
+// status: this pass's look-back words; status_next: the next pass's, of which
+// this tile clears its own (nullptr for the last pass)
+__global__ void __launch_bounds__(SORT_THREADS, 2) k_sort_pass(
     const unsigned long long *__restrict__ kin, const unsigned *__restrict__ vin, unsigned long long *__restrict__ kout,
     unsigned *__restrict__ vout, int n, int shift, int sys_mode, const int *__restrict__ poff, int S,
-    const unsigned *__restrict__ g_off, unsigned *status, unsigned *tile_counter, int *err)
+    const unsigned *__restrict__ g_off, unsigned *status, unsigned *status_next, unsigned *tile_counter, int *err)
 {
-    extern __shared__ unsigned long long s_keys[];             // SORT_TILE keys
-    unsigned *s_vals = (unsigned *)(s_keys + SORT_TILE);       // SORT_TILE values
-    unsigned char *s_dig = (unsigned char *)(s_vals + SORT_TILE);  // SORT_TILE digits
-    __shared__ unsigned s_whist[SORT_WARPS][RADIX];
-    __shared__ unsigned s_texcl[RADIX];
-    __shared__ unsigned s_gbase[RADIX];
-    __shared__ unsigned s_wsum[SORT_WARPS];
-    __shared__ int s_tile;
+    extern __shared__ __align__(16) unsigned char sort_smem_raw[];
+    SortSmem &sm = *reinterpret_cast<SortSmem *>(sort_smem_raw);
 
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    if (tid == 0) s_tile = (int)atomicAdd(tile_counter, 1u);
-    for (int i = tid; i < SORT_WARPS * RADIX; i += SORT_THREADS) (&s_whist[0][0])[i] = 0;
+    if (tid == 0) sm.tile = (int)atomicAdd(tile_counter, 1u);
+    for (int i = tid; i < SORT_WARPS * RADIX; i += SORT_THREADS) (&sm.whist[0][0])[i] = 0;
     __syncthreads();
-    const int tile = s_tile;
+    const int tile = sm.tile;
     const long long tile_base = (long long)tile * SORT_TILE;
     const long long wbase = tile_base + (long long)w * 32 * SORT_ITEMS;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -123,132 +163,144 @@ __global__ void __launch_bounds__(SORT_THREADS, 4) k_sort_pass(
     unsigned v[SORT_ITEMS], rank[SORT_ITEMS], dg[SORT_ITEMS];
 #pragma unroll
     for (int j = 0; j < SORT_ITEMS; j++) {
-        long long idx = wbase + j * 32 + lane;
-        bool valid = idx < n;
+        const long long idx = wbase + j * 32 + lane;
+        const bool valid = idx < n;
         k[j] = valid ? kin[idx] : ~0ull;
         v[j] = valid ? vin[idx] : 0u;
     }
 #pragma unroll
     for (int j = 0; j < SORT_ITEMS; j++) {
-        long long idx = wbase + j * 32 + lane;
+        const long long idx = wbase + j * 32 + lane;
         unsigned d;
-        if (idx >= n) d = 255u;
-        else if (sys_mode) d = ((unsigned)sort_sys_of(poff, S, v[j]) >> shift) & 255u;
-        else d = (unsigned)(k[j] >> shift) & 255u;
+        if (idx >= n) d = RADIX - 1;
+        else if (sys_mode) d = ((unsigned)sort_sys_of(poff, S, v[j]) >> shift) & (RADIX - 1);
+        else d = (unsigned)(k[j] >> shift) & (RADIX - 1);
         dg[j] = d;
     }
     // stable warp-level ranking in (item, lane) order == index order
 #pragma unroll
     for (int j = 0; j < SORT_ITEMS; j++) {
-        unsigned d = dg[j];
-        unsigned peers = __match_any_sync(0xffffffffu, d);
-        int leader = __ffs(peers) - 1;
+        const unsigned d = dg[j];
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const int leader = __ffs(peers) - 1;
         unsigned base = 0;
-        if (lane == leader) base = atomicAdd(&s_whist[w][d], (unsigned)__popc(peers));
+        if (lane == leader) base = atomicAdd(&sm.whist[w][d], (unsigned)__popc(peers));
         base = __shfl_sync(peers, base, leader);
         rank[j] = base + __popc(peers & lt_mask);
         __syncwarp();
     }
     __syncthreads();
 
-    // per digit: warp-exclusive offsets and the tile's count
-    const int d = tid;   // SORT_THREADS == RADIX
-    unsigned sum = 0;
+    // per digit (thread tid owns digits DPT*tid ..): warp-exclusive offsets and the tile's count
+    unsigned sum[DPT];
 #pragma unroll
-    for (int ww = 0; ww < SORT_WARPS; ww++) {
-        unsigned c = s_whist[ww][d];
-        s_whist[ww][d] = sum;
-        sum += c;
-    }
-    // publish and look back
-    unsigned *st = status + (size_t)tile * RADIX;
-    unsigned excl = 0;
-    if (tile == 0) {
-        st_status(&st[d], ST_INC | (sum & ST_VALUE));
-    } else {
-        st_status(&st[d], ST_AGG | (sum & ST_VALUE));
-        int t = tile - 1;
-        int spins = 0;
-        while (t >= 0) {
-            unsigned sv = ld_status(status + (size_t)t * RADIX + d);
-            if ((sv & ST_FLAGS) == 0u) {
-                if (++spins > GG_SORT_SPIN_LIMIT) {
-                    atomicOr(err, GG_EBIT_SORT_TIMEOUT);
-                    break;
-                }
-                __nanosleep(32);
-                continue;
-            }
-            excl += sv & ST_VALUE;
-            if ((sv & ST_FLAGS) == ST_INC) break;
-            t--;
+    for (int q = 0; q < DPT; q++) {
+        const int d = DPT * tid + q;
+        unsigned acc = 0;
+#pragma unroll
+        for (int ww = 0; ww < SORT_WARPS; ww++) {
+            const unsigned c = sm.whist[ww][d];
+            sm.whist[ww][d] = acc;
+            acc += c;
         }
-        st_status(&st[d], ST_INC | ((excl + sum) & ST_VALUE));
+        sum[q] = acc;
     }
-    s_gbase[d] = g_off[d] + excl;
+    // publish and look back, digit by digit
+    unsigned *st = status + (size_t)tile * RADIX;
+#pragma unroll
+    for (int q = 0; q < DPT; q++) {
+        const int d = DPT * tid + q;
+        unsigned excl = 0;
+        if (tile == 0) {
+            st_status(&st[d], ST_INC | (sum[q] & ST_VALUE));
+        } else {
+            st_status(&st[d], ST_AGG | (sum[q] & ST_VALUE));
+            int t = tile - 1;
+            int spins = 0;
+            while (t >= 0) {
+                const unsigned sv = ld_status(status + (size_t)t * RADIX + d);
+                if ((sv & ST_FLAGS) == 0u) {
+                    if (++spins > GG_SORT_SPIN_LIMIT) {
+                        atomicOr(err, GG_EBIT_SORT_TIMEOUT);
+                        break;
+                    }
+                    __nanosleep(32);
+                    continue;
+                }
+                excl += sv & ST_VALUE;
+                if ((sv & ST_FLAGS) == ST_INC) break;
+                t--;
+            }
+            st_status(&st[d], ST_INC | ((excl + sum[q]) & ST_VALUE));
+        }
+        sm.gbase[d] = g_off[d] + excl;
+        if (status_next) status_next[(size_t)tile * RADIX + d] = 0u;
+    }
 
     // exclusive scan of the tile's digit counts
-    unsigned x = sum;
-    for (int o = 1; o < 32; o <<= 1) {
-        unsigned y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
+    {
+        unsigned e[DPT];
+        block_excl_scan(sum, e, sm.wsum);
+#pragma unroll
+        for (int q = 0; q < DPT; q++) sm.texcl[DPT * tid + q] = e[q];
     }
-    if (lane == 31) s_wsum[w] = x;
-    __syncthreads();
-    unsigned wo = 0;
-    for (int ww = 0; ww < w; ww++) wo += s_wsum[ww];
-    s_texcl[d] = x - sum + wo;
     __syncthreads();
 
     // scatter into shared memory in digit order
 #pragma unroll
     for (int j = 0; j < SORT_ITEMS; j++) {
-        long long idx = wbase + j * 32 + lane;
+        const long long idx = wbase + j * 32 + lane;
         if (idx < n) {
-            unsigned dd = dg[j];
-            unsigned pos = s_texcl[dd] + s_whist[w][dd] + rank[j];
-            s_keys[pos] = k[j];
-            s_vals[pos] = v[j];
-            s_dig[pos] = (unsigned char)dd;
+            const unsigned dd = dg[j];
+            const unsigned pos = sm.texcl[dd] + sm.whist[w][dd] + rank[j];
+            sm.keys[pos] = k[j];
+            sm.vals[pos] = v[j];
+            sm.dig[pos] = (unsigned short)dd;
         }
     }
     __syncthreads();
-    long long rem = (long long)n - tile_base;
-    int nvalid = rem < SORT_TILE ? (int)rem : SORT_TILE;
+    const long long rem = (long long)n - tile_base;
+    const int nvalid = rem < SORT_TILE ? (int)rem : SORT_TILE;
     for (int i = tid; i < nvalid; i += SORT_THREADS) {
-        unsigned dd = s_dig[i];
-        unsigned gpos = s_gbase[dd] + (unsigned)i - s_texcl[dd];
+        const unsigned dd = sm.dig[i];
+        const unsigned gpos = sm.gbase[dd] + (unsigned)i - sm.texcl[dd];
         if (gpos < (unsigned)n) {   // always true unless a look-back gave up
-            kout[gpos] = s_keys[i];
-            vout[gpos] = s_vals[i];
+            kout[gpos] = sm.keys[i];
+            vout[gpos] = sm.vals[i];
         }
     }
 }
 
-size_t gg_sort_scratch_bytes(long long n, int npasses)
+static int sort_passes(int bits) { return bits <= 0 ? 0 : (bits + SORT_BITS - 1) / SORT_BITS; }
+
+// Scratch of a sort of n pairs, whatever the number of passes (at most
+// GG_SORT_MAX_PASSES), so that one buffer serves every sort of up to n pairs.
+size_t gg_sort_scratch_bytes(long long n)
 {
-    long long ntiles = (n + SORT_TILE - 1) / SORT_TILE;
+    const long long ntiles = (n + SORT_TILE - 1) / SORT_TILE;
     size_t b = 0;
     b += (size_t)n * 8 + 256;                                // alternate keys
     b += (size_t)n * 4 + 256;                                // alternate values
-    b += (size_t)npasses * RADIX * 4 * 2;                    // histograms + offsets
+    b += (size_t)GG_SORT_MAX_PASSES * RADIX * 4 * 2 + 512;   // histograms + offsets
     b += 256;                                                // tile counters
-    b += (size_t)npasses * ntiles * RADIX * 4 + 256;         // status words
+    b += 2 * ((size_t)ntiles * RADIX * 4 + 256);             // two arrays of status words
     return b;
 }
 
-static int sort_smem_bytes() { return SORT_TILE * (8 + 4 + 1); }
+static int sort_smem_bytes() { return (int)sizeof(SortSmem); }
 
-// Sorts (keys, vals) of length n.  nkey key passes (8 bits each, from bit 0),
-// then nsys system-id passes.  Scratch must be gg_sort_scratch_bytes(n, nkey+nsys)
-// bytes, 256-byte aligned.  The result is left in keys/vals.
-gg_status gg_sort_pairs_run(unsigned long long *keys, unsigned *vals, long long n, int nkey, int nsys,
+// Sorts (keys, vals) of length n by the low key_bits bits of the key, then
+// stably by the low sys_bits bits of each value's system id (the system whose
+// range [poff[s], poff[s+1]) holds the value).  Scratch must be
+// gg_sort_scratch_bytes(n) bytes, 256-byte aligned.  The
+// result is left in keys/vals.
+gg_status gg_sort_pairs_run(unsigned long long *keys, unsigned *vals, long long n, int key_bits, int sys_bits,
                             const int *poff, int S, void *scratch, int *err, cudaStream_t st)
 {
-    int np = nkey + nsys;
+    const int nkey = sort_passes(key_bits), nsys = sort_passes(sys_bits), np = nkey + nsys;
     if (np <= 0 || n <= 1) return GG_OK;
     if (np > GG_SORT_MAX_PASSES || n >= (1ll << 30)) return GG_ERR_TOO_LARGE;
-    long long ntiles = (n + SORT_TILE - 1) / SORT_TILE;
+    const long long ntiles = (n + SORT_TILE - 1) / SORT_TILE;
     char *p = (char *)scratch;
     auto take = [&](size_t bytes) {
         char *r = p;
@@ -260,32 +312,31 @@ gg_status gg_sort_pairs_run(unsigned long long *keys, unsigned *vals, long long 
     unsigned *hist = (unsigned *)take((size_t)np * RADIX * 4);
     unsigned *off = (unsigned *)take((size_t)np * RADIX * 4);
     unsigned *counters = (unsigned *)take(256);
-    unsigned *status = (unsigned *)take((size_t)np * ntiles * RADIX * 4);
+    unsigned *status[2] = {(unsigned *)take((size_t)ntiles * RADIX * 4), (unsigned *)take((size_t)ntiles * RADIX * 4)};
 
     GG_CUDA_TRY(cudaMemsetAsync(hist, 0, (size_t)np * RADIX * 4, st));
     GG_CUDA_TRY(cudaMemsetAsync(counters, 0, 256, st));
-    GG_CUDA_TRY(cudaMemsetAsync(status, 0, (size_t)np * ntiles * RADIX * 4, st));
+    GG_CUDA_TRY(cudaMemsetAsync(status[0], 0, (size_t)ntiles * RADIX * 4, st));
     {
         int threads = 256, blocks = gg_num_sms() * 4;
-        long long need = (n + threads - 1) / threads;
+        const long long need = (n + threads - 1) / threads;
         if (need < blocks) blocks = (int)need;
-        k_sort_hist<<<blocks, threads, 0, st>>>(keys, vals, (int)n, nkey, nsys, poff, S, hist);
-        k_sort_hist_scan<<<np, RADIX, 0, st>>>(hist, off);
+        const int hsmem = np * RADIX * 4;
+        GG_CUDA_TRY(cudaFuncSetAttribute(k_sort_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, hsmem));
+        k_sort_hist<<<blocks, threads, hsmem, st>>>(keys, vals, (int)n, nkey, nsys, poff, S, hist);
+        k_sort_hist_scan<<<np, SORT_THREADS, 0, st>>>(hist, off);
         gg_note_launches(2);
     }
-    static bool attr_set = false;
-    if (!attr_set) {
-        GG_CUDA_TRY(cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, sort_smem_bytes()));
-        attr_set = true;
-    }
+    // the attribute is per device: set it on every call (cheap)
+    GG_CUDA_TRY(cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, sort_smem_bytes()));
     unsigned long long *ka = keys, *kb = kalt;
     unsigned *va = vals, *vb = valt;
     for (int pass = 0; pass < np; pass++) {
-        int sys_mode = pass >= nkey;
-        int shift = sys_mode ? 8 * (pass - nkey) : 8 * pass;
+        const int sys_mode = pass >= nkey;
+        const int shift = sys_mode ? SORT_BITS * (pass - nkey) : SORT_BITS * pass;
         k_sort_pass<<<(unsigned)ntiles, SORT_THREADS, sort_smem_bytes(), st>>>(
-            ka, va, kb, vb, (int)n, shift, sys_mode, poff, S, off + pass * RADIX, status + (size_t)pass * ntiles * RADIX,
-            counters + pass, err);
+            ka, va, kb, vb, (int)n, shift, sys_mode, poff, S, off + pass * RADIX, status[pass & 1],
+            pass + 1 < np ? status[(pass + 1) & 1] : nullptr, counters + pass, err);
         gg_note_launches(1);
         unsigned long long *tk = ka; ka = kb; kb = tk;
         unsigned *tv = va; va = vb; vb = tv;
@@ -306,9 +357,9 @@ gg_status gg_sort_pairs_run(unsigned long long *keys, unsigned *vals, long long 
 gg_status gg_sort_timeout_selftest(cudaStream_t st)
 {
     const int n = 2 * SORT_TILE;
-    const size_t bytes = gg_sort_scratch_bytes(n, 1);
     char *base = nullptr;
-    GG_CUDA_TRY(cudaMallocAsync((void **)&base, bytes + 4 * (size_t)n * 12 + 1024, st));
+    const size_t bytes = (size_t)n * 24 + 2 * RADIX * 4 + RADIX * 4 + 4096;
+    GG_CUDA_TRY(cudaMallocAsync((void **)&base, bytes, st));
     char *p = base;
     auto take = [&](size_t b) { char *r = p; p += (b + 255) & ~(size_t)255; return (void *)r; };
     unsigned long long *kin = (unsigned long long *)take((size_t)n * 8);
@@ -322,13 +373,9 @@ gg_status gg_sort_timeout_selftest(cudaStream_t st)
     cudaMemsetAsync(base, 0, (size_t)(p - base), st);
     const unsigned one = 1;   // the CTA takes tile 1; tile 0 is never started
     cudaMemcpyAsync(counter, &one, sizeof one, cudaMemcpyHostToDevice, st);
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, sort_smem_bytes());
-        attr_set = true;
-    }
+    cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, sort_smem_bytes());
     k_sort_pass<<<1, SORT_THREADS, sort_smem_bytes(), st>>>(kin, vin, kout, vout, n, 0, 0, nullptr, 1, off, status,
-                                                             counter, err);
+                                                             nullptr, counter, err);
     gg_note_launches(1);
     int herr = 0;
     cudaError_t e = cudaGetLastError();

@@ -187,9 +187,9 @@ gg_status gg_order_groups_by_cost(const GGGroup *groups, const int *ngroups, int
     const int blocks = std::max(1, std::min(gg_num_sms() * 4, (maxg + 255) / 256));
     k_group_cost<<<blocks, 256, 0, st>>>(groups, ngroups, maxg, tlist, perm, cost, key, gorder);
     gg_note_launches(1);
-    // one 8-bit pass; the sort is stable, so the groups of one cost octave keep
+    // one pass over the 8-bit key; the sort is stable, so the groups of one cost octave keep
     // target order and neighbouring warps still walk neighbouring regions
-    return gg_sort_pairs_run(key, gorder, maxg, 1, 0, nullptr, 1, sort_scratch, err, st);
+    return gg_sort_pairs_run(key, gorder, maxg, 8, 0, nullptr, 1, sort_scratch, err, st);
 }
 
 // ---- active targets ------------------------------------------------------------
@@ -298,6 +298,95 @@ void gg_launch_direct(long long n_src, const double *pos, const double *mass, co
     long long blocks = (n_tgt + DS_TILE - 1) / DS_TILE;
     if (blocks < 1) return;
     k_direct<<<(unsigned)blocks, DS_TILE, 0, st>>>(n_src, pos, mass, h, n_tgt, targets, acc, pot);
+    gg_note_launches(1);
+}
+
+// FP64 direct sum of sampled targets against the sources of their own system,
+// read from the load-order records (masses and softenings as stored, FP32):
+// the force and potential a sampled target would have with every node opened,
+// and its stored mass.
+// One block per target, the sources strided over the block and the sums
+// reduced in a fixed order, so the result does not depend on scheduling.
+// Used by the autotuner to measure a configuration's force errors.
+#define DR_THREADS 256
+__global__ void __launch_bounds__(DR_THREADS) k_direct_records(const GGPart *__restrict__ rec,
+                                                               const int *__restrict__ poff,
+                                                               const int2 *__restrict__ tg, int ntg,
+                                                               double *__restrict__ acc, double *__restrict__ pot,
+                                                               double *__restrict__ mass)
+{
+    __shared__ double red[4][DR_THREADS];
+    for (int t = blockIdx.x; t < ntg; t += gridDim.x) {
+        const int i = tg[t].x, s = tg[t].y;
+        const GGPart q = rec[i];
+        const double hi = (double)q.h;
+        double ax = 0, ay = 0, az = 0, pp = 0;
+        for (int j = poff[s] + threadIdx.x; j < poff[s + 1]; j += DR_THREADS) {
+            const GGPart r = rec[j];
+            const double dx = r.x - q.x, dy = r.y - q.y, dz = r.z - q.z;
+            const double r2 = dx * dx + dy * dy + dz * dz, mj = (double)r.m;
+            if (r2 > 0 && mj > 0) {
+                const double rr = sqrt(r2), hj = (double)r.h;
+                double fac, fp;
+                if (rr >= hi && rr >= hj) {
+                    fac = mj / (r2 * rr);
+                    fp = -mj / rr;
+                } else {
+                    const double hg = hi > hj ? hi : hj, hinv = 1.0 / hg;
+                    double wf, wp;
+                    spline64(rr * hinv, hinv, &wf, &wp);
+                    fac = mj * wf;
+                    fp = mj * wp;
+                }
+                ax += dx * fac; ay += dy * fac; az += dz * fac; pp += fp;
+            }
+        }
+        red[0][threadIdx.x] = ax; red[1][threadIdx.x] = ay; red[2][threadIdx.x] = az; red[3][threadIdx.x] = pp;
+        __syncthreads();
+        for (int w = DR_THREADS / 2; w > 0; w >>= 1) {
+            if ((int)threadIdx.x < w)
+                for (int k = 0; k < 4; k++) red[k][threadIdx.x] += red[k][threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            acc[3 * (size_t)t] = red[0][0]; acc[3 * (size_t)t + 1] = red[1][0]; acc[3 * (size_t)t + 2] = red[2][0];
+            pot[t] = red[3][0];
+            mass[t] = (double)q.m;
+        }
+        __syncthreads();
+    }
+}
+
+// rows of an output (acc n*3, pot n; load order, or active order) gathered
+// for the sampled targets (tg[t].x = the row)
+__global__ void k_gather_rows(const double *__restrict__ acc, const double *__restrict__ pot,
+                              const int2 *__restrict__ tg, int ntg, double *__restrict__ acc_out,
+                              double *__restrict__ pot_out)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntg; t += gridDim.x * blockDim.x) {
+        const size_t i = (size_t)tg[t].x;
+        acc_out[3 * (size_t)t] = acc[3 * i];
+        acc_out[3 * (size_t)t + 1] = acc[3 * i + 1];
+        acc_out[3 * (size_t)t + 2] = acc[3 * i + 2];
+        pot_out[t] = pot ? pot[i] : 0.0;
+    }
+}
+
+void gg_launch_direct_records(const GGPart *rec, const int *poff, const int2 *tg, int ntg, double *acc, double *pot,
+                              double *mass, cudaStream_t st)
+{
+    if (ntg < 1) return;
+    const int blocks = std::min(ntg, gg_num_sms() * 8);
+    k_direct_records<<<blocks, DR_THREADS, 0, st>>>(rec, poff, tg, ntg, acc, pot, mass);
+    gg_note_launches(1);
+}
+
+void gg_launch_gather_rows(const double *acc, const double *pot, const int2 *tg, int ntg, double *acc_out,
+                           double *pot_out, cudaStream_t st)
+{
+    if (ntg < 1) return;
+    const int blocks = std::min((ntg + 255) / 256, gg_num_sms() * 4);
+    k_gather_rows<<<blocks, 256, 0, st>>>(acc, pot, tg, ntg, acc_out, pot_out);
     gg_note_launches(1);
 }
 
@@ -410,11 +499,11 @@ gg_status gg_order_targets_by_softening(int nt, const int *tlist_in, const int *
     int sbits = 0;
     while ((1 << sbits) < S) sbits++;
     const int lmax = std::min(GG_ORDER_MAX_LEVEL, (64 - 8 - sbits) / 3);
-    const int np = (sbits + 3 * lmax + 8 + 7) / 8;
+    const int key_bits = sbits + 3 * lmax + 8;
     int blocks = gg_num_sms() * 4;
     k_target_keys<<<blocks, 256, 0, st>>>(nt, tlist_in, parts, pkeys, poff, S, dom, hmm, lmax, key, val);
     gg_note_launches(1);
-    gg_status s = gg_sort_pairs_run(key, val, nt, np, 0, nullptr, 1, sort_scratch, err, st);
+    gg_status s = gg_sort_pairs_run(key, val, nt, key_bits, 0, nullptr, 1, sort_scratch, err, st);
     if (s) return s;
     k_target_apply<<<blocks, 256, 0, st>>>(nt, val, tlist_in, tout_in, tlist_out, tout_out);
     gg_note_launches(1);

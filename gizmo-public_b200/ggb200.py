@@ -119,8 +119,10 @@ def load_library():
             "gg_load_velocities": (i32, [P, P, i64]),
             "gg_load_velocities_device": (i32, [P, P]),
             "gg_drift": (i32, [P, dbl]),
+            "gg_set_positions": (i32, [P, P, i64]),
             "gg_device_bytes": (i32, [P, ctypes.POINTER(i64)]),
             "gg_get_order": (i32, [P, P]),
+            "gg_get_order_device": (i32, [P, P]),
             "gg_evaluate_potential": (i32, [P, P, i64, P, dbl, dbl, P, ctypes.POINTER(Stats)]),
             "gg_evaluate_potential_device": (i32, [P, P, i64, P, dbl, dbl, P]),
             "gg_energy_device": (i32, [P, P, P, P]),
@@ -134,6 +136,8 @@ def load_library():
             "gg_graph_capture_step": (i32, [P, dbl, dbl, P, P]),
             "gg_graph_launch": (i32, [P]),
             "gg_autotune": (i32, [P, dbl, dbl, ctypes.POINTER(Config), ctypes.POINTER(dbl)]),
+            "gg_tune_accuracy": (i32, [P, dbl, dbl, ctypes.POINTER(Config), ctypes.POINTER(i32)]),
+            "gg_autotune_active": (i32, [P, P, i64, dbl, dbl, ctypes.POINTER(Config), ctypes.POINTER(dbl)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -365,6 +369,10 @@ class GravityTree:
         _check(self._lib.gg_get_order(self._h, out.ctypes.data), "gg_get_order")
         return out
 
+    def order_device(self, d_order):
+        """The same order into a device int32 tensor of N entries (asynchronous)."""
+        _check(self._lib.gg_get_order_device(self._h, _ptr(d_order)), "gg_get_order_device")
+
     def device_bytes(self):
         """Device memory the context holds now."""
         v = ctypes.c_int64()
@@ -380,6 +388,13 @@ class GravityTree:
             d = np.ascontiguousarray(dt, dtype=np.float64)
             _check(self._lib.gg_drift_systems(self._h, d.ctypes.data), "gg_drift_systems")
 
+    def set_positions(self, pos):
+        """The particles' current positions (N,3, load order) replace the
+        resident ones; the tree and its nodes stay (call drift first for the
+        nodes)."""
+        p = np.ascontiguousarray(pos, dtype=np.float64)
+        _check(self._lib.gg_set_positions(self._h, p.ctypes.data, 24), "gg_set_positions")
+
     def capture_step(self, d_acc, d_pot=None, err_tol_force_acc=0.0025, err_tol_theta=0.0):
         """Capture build + walk of every resident system as one CUDA graph (the
         context needs its own stream, see set_stream, and one uncaptured step)."""
@@ -390,15 +405,40 @@ class GravityTree:
         """Replay the captured step on the context's stream (asynchronous)."""
         _check(self._lib.gg_graph_launch(self._h), "gg_graph_launch")
 
-    def autotune(self, err_tol_force_acc=0.0025, err_tol_theta=0.0):
+    def autotune(self, err_tol_force_acc=0.0025, err_tol_theta=0.0, d_active=None, n_active=0):
         """Pick leaf size, group size, blocks per SM, flush threshold and node
-        staging by timing the walk of the resident systems; returns (config dict, ms)."""
+        staging by timing the walk of the resident systems (of the active
+        targets d_active, a device int32 tensor, when given), refusing any
+        candidate less accurate than the context's configuration; returns
+        (config dict, ms)."""
         cfg = Config()
         ms = ctypes.c_double()
-        _check(self._lib.gg_autotune(self._h, err_tol_force_acc, err_tol_theta, ctypes.byref(cfg), ctypes.byref(ms)),
-               "gg_autotune")
+        if d_active is None:
+            _check(self._lib.gg_autotune(self._h, err_tol_force_acc, err_tol_theta, ctypes.byref(cfg),
+                                         ctypes.byref(ms)), "gg_autotune")
+        else:
+            _check(self._lib.gg_autotune_active(self._h, _ptr(d_active), int(n_active), err_tol_force_acc,
+                                                err_tol_theta, ctypes.byref(cfg), ctypes.byref(ms)),
+                   "gg_autotune_active")
         return dict(leaf_size=cfg.leaf_size, group_size=cfg.group_size, flush=cfg.flush_threshold,
                     blocks_per_sm=cfg.walk_blocks_per_sm, node_staging=cfg.node_staging), ms.value
+
+    def tune_accuracy(self, err_tol_force_acc=0.0025, err_tol_theta=0.0, **candidate):
+        """The autotuner's accuracy gate for one candidate configuration
+        (leaf_size, group_size, flush, blocks_per_sm, node_staging, target_order,
+        group_order; unset fields keep the context's defaults) against this
+        context's own: True if the candidate passes."""
+        cfg = Config()
+        self._lib.gg_config_default(ctypes.byref(cfg))
+        names = {"leaf_size": "leaf_size", "group_size": "group_size", "flush": "flush_threshold",
+                 "blocks_per_sm": "walk_blocks_per_sm", "node_staging": "node_staging",
+                 "target_order": "target_order", "group_order": "group_order"}
+        for k, v in candidate.items():
+            setattr(cfg, names[k], int(v))
+        ok = ctypes.c_int32()
+        _check(self._lib.gg_tune_accuracy(self._h, err_tol_force_acc, err_tol_theta, ctypes.byref(cfg),
+                                          ctypes.byref(ok)), "gg_tune_accuracy")
+        return bool(ok.value)
 
 
 def gravity_tree(pos, mass, h, G=1.0, err_tol_force_acc=0.0025, err_tol_theta=0.7, active=None, tree=None,

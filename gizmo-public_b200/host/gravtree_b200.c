@@ -16,9 +16,10 @@
  * (the FirstActiveParticle / NextActiveParticle chain, run.c:473-496).
  * Between rebuilds the reference's walk drifts particles and nodes to the
  * current time itself (drift_particle and force_drift_node, called lazily at
- * forcetree.c:1841 and :2051-2057); here the resident device tree is drifted
- * instead, with the current P[].Vel, over the interval since the previous
- * walk.  Single MPI rank per GPU.
+ * forcetree.c:1841 and :2051-2057); here the resident device tree's nodes are
+ * drifted instead, with the current P[].Vel, over the interval since the
+ * previous walk, and its particles take the current P[].Pos.  Single MPI rank
+ * per GPU.
  */
 #include <math.h>
 #include <stdio.h>
@@ -80,11 +81,16 @@ void gravtree_b200_build(void)
     gg_tree_ti = All.Ti_Current;
 }
 
-/* Bring the resident tree to All.Ti_Current without a rebuild: particles move
- * by Vel*dt (predict.c:97-137), nodes by force_drift_node
- * (forcetree_update.c:265-338).  Velocities do not change between two walks
- * (kicks come after the force computation), so one drift per walk interval
- * with the current velocities follows the reference's drift. */
+/* Bring the resident tree to All.Ti_Current without a rebuild: nodes move by
+ * force_drift_node (forcetree_update.c:265-338) with the current velocities,
+ * and the particles take their current P[].Pos.  The reference's walk reads
+ * P[].Pos, which drift_particle (predict.c:97-137) has already brought to the
+ * current time -- by Vel*dt for most particles, but by each build's own rule
+ * where there is one (advect_mesh_point for MFV cells, super-timestepped
+ * binaries, frozen hydro) -- so the positions are taken from P[] rather than
+ * drifted here.  Velocities do not change between two walks (kicks come after
+ * the force computation), so one node drift per walk interval with the
+ * current velocities follows the reference's lazy node drift. */
 static void gravtree_b200_drift(void)
 {
     gg_status st;
@@ -94,6 +100,8 @@ static void gravtree_b200_drift(void)
     st = gg_load_velocities(gg_tree_ctx, &P[0].Vel[0], (int64_t)sizeof(struct particle_data));
     if (st) gg_fail("gg_load_velocities", st);
     if ((st = gg_drift(gg_tree_ctx, dt))) gg_fail("gg_drift", st);
+    st = gg_set_positions(gg_tree_ctx, &P[0].Pos[0], (int64_t)sizeof(struct particle_data));
+    if (st) gg_fail("gg_set_positions", st);
     gg_tree_ti = All.Ti_Current;
 }
 
@@ -197,28 +205,4 @@ double gravtree_b200_walk(void)
 #endif
     }
     return (double)stats.interactions;
-}
-
-/* The whole of gravity_tree() for an isolated, tree-only, single-rank run:
- * build when TreeReconstructFlag is set (gravtree.c:67-78), walk, then the
- * reference's post-processing for this configuration (gravtree.c:475-522):
- * switch to the relative criterion, multiply by G, OldAcc = |a|/G. */
-double gravity_tree_b200(void)
-{
-    int i, j;
-    if (TreeReconstructFlag) {
-        gravtree_b200_build();
-        TreeReconstructFlag = 0;
-    }
-    double cost = gravtree_b200_walk();
-    if (All.TypeOfOpeningCriterion == 1) All.ErrTolTheta = 0;
-    for (i = FirstActiveParticle; i >= 0; i = NextActiveParticle[i]) {
-        for (j = 0; j < 3; j++) P[i].GravAccel[j] *= All.G;
-#ifdef EVALPOTENTIAL
-        P[i].Potential *= All.G;
-#endif
-        double ax = P[i].GravAccel[0], ay = P[i].GravAccel[1], az = P[i].GravAccel[2];
-        P[i].OldAcc = sqrt(ax * ax + ay * ay + az * az) / All.G;
-    }
-    return cost;
 }

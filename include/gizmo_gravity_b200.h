@@ -133,6 +133,10 @@ gg_status gg_get_domains(gg_ctx *ctx, gg_domain *out);
  * 21 bits per dimension; the reference orders particles that share a 21-bit
  * cell by its finer key bits.  Blocking. */
 gg_status gg_get_order(gg_ctx *ctx, int32_t *order_out);
+/* The same order into device memory, asynchronous on the context's stream
+ * (a split of one system over several GPUs cuts it into Peano-Hilbert ranges
+ * of targets, the way domain.c:2224-2300 cuts the curve into domains). */
+gg_status gg_get_order_device(gg_ctx *ctx, int32_t *d_order_out);
 
 /* ---- walk --------------------------------------------------------------
  * The force_treeevaluate loop of gravity_tree (gravtree.c:138-457).
@@ -199,6 +203,17 @@ gg_status gg_load_velocities(gg_ctx *ctx, const double *vel, int64_t vel_stride_
 gg_status gg_load_velocities_device(gg_ctx *ctx, const double *d_vel);
 gg_status gg_drift(gg_ctx *ctx, double dt);
 gg_status gg_drift_systems(gg_ctx *ctx, const double *dt);
+/* The particles' current positions (load order, host, strided like
+ * gg_load_particles) replace the resident ones without a rebuild; nodes are
+ * left as they are.  For callers whose particles do not all move by Vel*dt
+ * between rebuilds: the reference's walk reads P[].Pos, which drift_particle
+ * (predict.c:97-137) advances by each build's own rule (advect_mesh_point for
+ * MFV cells, super-timestepped binaries, frozen hydro), so GIZMO calls
+ * gg_drift (nodes, by force_drift_node) and then gg_set_positions(P[].Pos).
+ * A non-finite position makes the next evaluation return GG_ERR_BAD_INPUT.
+ * Asynchronous on the context's stream (the host array has been read when it
+ * returns). */
+gg_status gg_set_positions(gg_ctx *ctx, const double *pos, int64_t pos_stride_bytes);
 
 /* ---- batches of independent systems and asynchronous evaluation ----------
  * No counterpart in the reference, which holds one system per process.
@@ -237,13 +252,34 @@ gg_status gg_fetch_results(gg_ctx *ctx, double *acc_out, double *pot_out, gg_sta
 gg_status gg_graph_capture_step(gg_ctx *ctx, double err_tol_force_acc, double err_tol_theta, double *d_acc_out,
                                 double *d_pot_out);
 gg_status gg_graph_launch(gg_ctx *ctx);
-/* Times the walk of the resident systems over leaf size {8,16}, group size
- * {32,64}, blocks per SM {2,3} and flush threshold {64,96}, each trial from the
- * same OldAcc, keeps the fastest in the context (rebuilding the tree with its
- * leaf size) and returns it in *chosen and its walk time in *best_ms
- * (nullable).  Synchronises. */
+/* Times the walk of the resident systems with the context's configuration
+ * and over leaf size {8,16}, group size {32,64}, blocks per SM {2,3} and flush
+ * threshold {64,128}, then the other node staging on the winner, each trial
+ * from the same OldAcc, and keeps the fastest configuration that passes the
+ * accuracy gate (rebuilding the tree with its leaf size); returns it in
+ * *chosen and its walk time in *best_ms (nullable).  The gate: on a fixed
+ * sample of targets (every target of a system of up to 2,048 particles, else
+ * 16,384 / n_systems evenly spaced ones, at least 64 and at most 4,096)
+ * against their FP64 direct sums, a candidate's
+ * 99th-percentile relative force error must be at most 1.1x the context's own
+ * configuration's in every system (plus 1e-7), and its sample potential energy
+ * 1/2 sum m phi no further from the direct sum's than 1.1x the context's own,
+ * or within 1e-5 relative; so a faster configuration is never taken at the
+ * price of accuracy.  No counterpart in the reference.  Synchronises. */
 gg_status gg_autotune(gg_ctx *ctx, double err_tol_force_acc, double err_tol_theta, gg_config *chosen,
                       double *best_ms);
+/* The same search for the walk of an active subset (device indices in load
+ * order, as gg_evaluate_device takes them): individual timesteps walk sparser
+ * groups of targets, whose best configuration differs from the all-target
+ * walk's.  The gate's sample is drawn from the active targets. */
+gg_status gg_autotune_active(gg_ctx *ctx, const int32_t *d_active, int64_t n_active, double err_tol_force_acc,
+                             double err_tol_theta, gg_config *chosen, double *best_ms);
+/* The accuracy gate of gg_autotune for one candidate configuration (leaf and
+ * group size, flush threshold, blocks per SM, node staging, target and group
+ * order) against the context's own, from the same OldAcc: *accepted = 1 if it
+ * passes, else 0.  The context is left as it was.  Synchronises. */
+gg_status gg_tune_accuracy(gg_ctx *ctx, double err_tol_force_acc, double err_tol_theta, const gg_config *candidate,
+                           int32_t *accepted);
 
 /* ---- kernel-level entry points (device pointers, cudaStream_t or NULL) ---- */
 /* domain_double_to_int (domain.c:2504-2513) + peano_hilbert_key (peano.c:303-319)
@@ -264,8 +300,12 @@ gg_status gg_radix_sort_pairs(int64_t n, uint64_t *d_keys, uint32_t *d_vals, int
  * loads the library until the process exits), so n is limited to
  * GG_NOALLOC_SORT_MAX_N; larger n returns GG_ERR_TOO_LARGE.  The first call on
  * a device looks up the array's device address; make that first call before
- * any stream capture.  All calls share the array: calls whose work overlaps
- * on the GPU race and must not be issued.  Blocking (synchronises `stream`). */
+ * any stream capture.  The address is kept for the life of the process, so
+ * after a cudaDeviceReset by the application the function must not be called
+ * again.  d_keys and d_vals must be device memory of the current device
+ * (GG_ERR_INVALID otherwise).  All calls share the array: calls whose work
+ * overlaps on the GPU race and must not be issued.  Blocking (synchronises
+ * `stream`). */
 #define GG_NOALLOC_SORT_MAX_N (1 << 20)
 gg_status gg_radix_sort_pairs_noalloc(int64_t n, uint64_t *d_keys, uint32_t *d_vals, int32_t key_bits, void *stream);
 /* Self-test of the library's only device-side wait, the radix sort's

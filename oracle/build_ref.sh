@@ -15,7 +15,7 @@ CC=/usr/bin/gcc
 # x86-64-v3 (AVX2/FMA): the binary runs on the GPU hosts as well as here
 CFLAGS="-O3 -march=x86-64-v3 -fopenmp -std=gnu99 -w"
 if [ ! -d "$REF" ]; then echo "reference tree not found: $REF" >&2; exit 1; fi
-if [ -x "$OUT/gizmo_ref" ] && [ -x "$OUT/gizmo_ref_pot" ] && [ -x "$OUT/gizmo_b200" ] && [ "$OUT/gizmo_b200" -nt "$HERE/ref_main.c" ] && [ "$OUT/gizmo_b200" -nt "$0" ] && [ "$OUT/gizmo_b200" -nt "$HERE/../gizmo-public_b200/host/gravtree_b200.c" ] && [ "$OUT/gizmo_b200" -nt "$HERE/../include/gizmo_gravity_b200.h" ] && [ "$OUT/gizmo_ref_pot" -nt "$HERE/ref_main.c" ]; then
+if [ -x "$OUT/gizmo_ref" ] && [ -x "$OUT/gizmo_ref_pot" ] && [ -x "$OUT/gizmo_b200" ] && [ "$OUT/gizmo_b200" -nt "$HERE/ref_main.c" ] && [ "$OUT/gizmo_b200" -nt "$0" ] && [ "$OUT/gizmo_b200" -nt "$HERE/../gizmo-public_b200/host/gravtree_b200.c" ] && [ "$OUT/gizmo_b200" -nt "$HERE/../include/gizmo_gravity_b200.h" ] && [ "$OUT/gizmo_b200" -nt "$HERE/patch_gravtree.py" ] && [ "$OUT/gizmo_ref_pot" -nt "$HERE/ref_main.c" ]; then
   echo "oracle/_ref/gizmo_ref is up to date"; exit 0
 fi
 MIRROR="$(mktemp -d /tmp/gg_ref_src.XXXXXX)"
@@ -76,12 +76,26 @@ xargs -P "$(nproc)" -I{} bash -c '{}' < "$MIRROR/cmds_pot.sh"
 $CC $CFLAGS -DGG_WITH_COMPUTE_POTENTIAL -I"$HERE/shim" -I"$MIRROR_POT" -c "$HERE/ref_main.c" -o "$OUT/obj_pot/ref_main.o"
 $CC $CFLAGS -o "$OUT/gizmo_ref_pot" $OBJS_POT "$OUT/obj_pot/ref_main.o" "$OUT/obj/mpi_single.o" "$OUT/obj/gsl_shim.o" -lm
 echo "built $OUT/gizmo_ref_pot"
-# GIZMO driving the B200 library through its C host code (needs the CUDA library)
+# GIZMO driving the B200 library: the reference's own gravity/gravtree.c with
+# the GRAVITY_GPU_B200 blocks of INTEGRATION.md added by patch_gravtree.py
+# (written into a third mirror, over its symlink), compiled with
+# -DGRAVITY_GPU_B200 and linked with the C host code
+# (gizmo-public_b200/host/gravtree_b200.c) and the CUDA library
 PKG="$(cd "$HERE/../gizmo-public_b200" && pwd)"
 if [ -f "$PKG/libgizmo_gravity_b200.so" ]; then
+  MIRROR_B200="$MIRROR/b200_tree"
+  mkdir -p "$MIRROR_B200"
+  cp -rs "$REF/." "$MIRROR_B200/"
+  rm -f "$MIRROR_B200/GIZMO_config.h"
+  cp "$HERE/shim/GIZMO_config.h" "$MIRROR_B200/GIZMO_config.h"
+  python3 "$HERE/patch_gravtree.py" "$REF/gravity/gravtree.c" "$MIRROR_B200/gravity/gravtree.c"
+  (cd "$MIRROR_B200" && $CC $CFLAGS -DGRAVITY_GPU_B200 -I"$HERE/shim" -I"$MIRROR_B200" -c gravity/gravtree.c \
+      -o "$OUT/obj/gravity_gravtree_b200.o")
+  OBJS_B200="$(echo $OBJS | tr ' ' '\n' | grep -v '/gravity_gravtree\.o$' | tr '\n' ' ')"
   $CC $CFLAGS -DGG_USE_B200 -I"$HERE/shim" -I"$MIRROR" -c "$HERE/ref_main.c" -o "$OUT/obj/ref_main_b200.o"
   $CC $CFLAGS -I"$HERE/shim" -I"$MIRROR" -I"$PKG/../include" -c "$PKG/host/gravtree_b200.c" -o "$OUT/obj/gravtree_b200.o"
-  $CC $CFLAGS -o "$OUT/gizmo_b200" $OBJS "$OUT/obj/ref_main_b200.o" "$OUT/obj/gravtree_b200.o" \
-      "$OUT/obj/mpi_single.o" "$OUT/obj/gsl_shim.o" -L"$PKG" -lgizmo_gravity_b200 -Wl,-rpath,'$ORIGIN/../../gizmo-public_b200' -lm
+  $CC $CFLAGS -o "$OUT/gizmo_b200" $OBJS_B200 "$OUT/obj/gravity_gravtree_b200.o" "$OUT/obj/ref_main_b200.o" \
+      "$OUT/obj/gravtree_b200.o" "$OUT/obj/mpi_single.o" "$OUT/obj/gsl_shim.o" -L"$PKG" -lgizmo_gravity_b200 \
+      -Wl,-rpath,'$ORIGIN/../../gizmo-public_b200' -lm
   echo "built $OUT/gizmo_b200"
 fi

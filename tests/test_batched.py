@@ -110,8 +110,33 @@ def test_autotune_keeps_the_force_error_and_returns_a_valid_config():
         torch.cuda.synchronize()
         assert t.last_stats()["error_word"] == 0
         tuned = _per_system_p99(ic, acc.cpu().numpy())
-        assert tuned < 2e-3 and tuned <= 1.5 * base + 1e-4
+        # the accuracy gate holds every system to 1.1x the base configuration
+        # on its own sample; on this independent sample allow sampling noise
+        assert tuned < 2e-3 and tuned <= 1.25 * base + 1e-5
         t.close()
+
+
+def test_tuner_gate_refuses_a_less_accurate_configuration():
+    """Leaf buckets of 16 on the reference's clustered golden put the potential
+    energy further from the direct sum than the reference tree does (and than
+    the default leaf 8): the autotuner's gate refuses it, while configurations
+    that change no opening decision (flush threshold, blocks per SM, node
+    staging) pass."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "clustered_1500.npz"))
+    tol = float(g["tol"])
+    with ggb200.GravityTree() as t:
+        t.load(g["pos"], g["mass"], g["h"])
+        t.build()
+        a1, _, _, _ = t.evaluate(err_tol_theta=0.7)
+        t.evaluate(old_acc=np.linalg.norm(a1, axis=1), err_tol_force_acc=tol)
+        assert not t.tune_accuracy(err_tol_force_acc=tol, leaf_size=16)
+        assert t.tune_accuracy(err_tol_force_acc=tol, flush=64)
+        assert t.tune_accuracy(err_tol_force_acc=tol, blocks_per_sm=3, node_staging=1)
+        # the context is left as it was: the same walk gives the same bits
+        a2, p2, _, _ = t.evaluate(old_acc=np.linalg.norm(a1, axis=1), err_tol_force_acc=tol)
+        a3, p3, _, _ = t.evaluate(old_acc=np.linalg.norm(a1, axis=1), err_tol_force_acc=tol)
+        assert np.array_equal(a2, a3) and np.array_equal(p2, p3)
 
 
 def test_split_system_step_on_one_gpu_equals_plain_evaluation():
@@ -144,3 +169,31 @@ def test_split_system_step_on_one_gpu_equals_plain_evaluation():
         assert torch.equal(acc_a, acc_b) and torch.equal(pot_a, pot_b)
         ta.close()
         tb.close()
+
+
+def test_autotune_for_an_active_subset():
+    """The search on the walk of a 10% active subset (individual timesteps):
+    a valid configuration, and the subset's forces with it stay within the
+    default configuration's error against the FP64 direct sum."""
+    import torch
+    ic = ics.clustered(200000, seed=17, n_clumps=40)
+    n = ic["pos"].shape[0]
+    act = ics.random_active(n, 0.1, seed=18).astype(np.int32)
+    tg = act[:: 16]
+    acc_d, _ = oracle.direct_sum(ic["pos"], ic["mass"], ic["h"], targets=tg)
+    rows = np.searchsorted(act, tg)
+    with ggb200.GravityTree() as t:
+        t.load(ic["pos"], ic["mass"], ic["h"])
+        t.build()
+        a1, _, _, _ = t.evaluate(err_tol_theta=0.7)
+        old = np.linalg.norm(a1, axis=1)
+        base, _, _, _ = t.evaluate(active=act, old_acc=old, err_tol_force_acc=0.001)
+        d_act = torch.from_numpy(act).cuda()
+        cfg, ms = t.autotune(err_tol_force_acc=0.001, d_active=d_act, n_active=act.size)
+        assert cfg["leaf_size"] in (8, 16) and cfg["group_size"] in (32, 64) and ms > 0
+        t.build()
+        tuned, _, _, st = t.evaluate(active=act, old_acc=old, err_tol_force_acc=0.001)
+    assert st["error_word"] == 0
+    b50, b99, _ = ics.error_stats(base[rows], acc_d)
+    t50, t99, _ = ics.error_stats(tuned[rows], acc_d)
+    assert t99 <= 1.25 * b99 + 1e-5, (t99, b99)

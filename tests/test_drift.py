@@ -122,3 +122,59 @@ def test_drift_rejects_missing_state_and_bad_steps():
         t.build()
         with pytest.raises(ggb200.GravityError):
             t.drift(0.01)
+
+
+def test_set_positions_with_the_drifted_positions_changes_nothing():
+    """gg_set_positions with the positions gg_drift computes (x + v*dt, each
+    operation rounded) leaves every result bitwise as it was."""
+    ic = ics.plummer(5000, seed=311)
+    old = _old(ic)
+    dt = 0.003
+    res = []
+    for reload in (False, True):
+        with ggb200.GravityTree() as t:
+            t.load(ic["pos"], ic["mass"], ic["h"])
+            t.load_velocities(ic["vel"])
+            t.build()
+            t.drift(dt)
+            if reload:
+                t.set_positions(ic["pos"] + ic["vel"] * dt)
+            res.append(t.evaluate(old_acc=old, want_ninter=True))
+    assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
+    assert np.array_equal(res[0][2], res[1][2])
+
+
+def test_set_positions_are_the_positions_the_walk_reads():
+    """Particles that moved by another rule than Vel*dt (as GIZMO's MFV cells
+    do): after gg_drift the caller's positions replace them, for targets and
+    sources alike.  With every node opened (relative criterion, OldAcc 0) the
+    walk is a direct sum at the caller's positions."""
+    ic = ics.plummer(3000, seed=312)
+    dt = 0.01
+    rng = np.random.default_rng(313)
+    moved = ic["pos"] + ic["vel"] * dt
+    odd = rng.random(3000) < 0.2
+    moved[odd] += rng.normal(scale=0.02, size=(int(odd.sum()), 3))
+    acc_d, _ = oracle.direct_sum(moved, ic["mass"], ic["h"])
+    with ggb200.GravityTree() as t:
+        t.load(ic["pos"], ic["mass"], ic["h"])
+        t.load_velocities(ic["vel"])
+        t.build()
+        t.drift(dt)
+        t.set_positions(moved)
+        a, _, _, st = t.evaluate(old_acc=np.zeros(3000), err_tol_theta=0.0)
+    assert st["error_word"] == 0
+    assert np.allclose(a, acc_d, rtol=1e-4, atol=1e-6 * np.abs(acc_d).max())
+
+
+def test_set_positions_refuses_non_finite():
+    ic = ics.plummer(1000, seed=314)
+    bad = ic["pos"].copy()
+    bad[7, 2] = np.inf
+    with ggb200.GravityTree() as t:
+        t.load(ic["pos"], ic["mass"], ic["h"])
+        t.build()
+        t.set_positions(bad)
+        with pytest.raises(ggb200.GravityError) as ei:
+            t.evaluate(err_tol_theta=0.7)
+        assert ei.value.status == -7

@@ -1,15 +1,21 @@
 """GIZMO itself driving the B200 library through its C host code.
 
 oracle/_ref/gizmo_b200 is the reference code (begrun, domain decomposition,
-the two start-up gravity passes of compute_grav_accelerations) with the tree
-construction and walk of gravity_tree() replaced by
-gizmo-public_b200/host/gravtree_b200.c, which hands GIZMO's own P[] records
-(strided) to the C ABI.  The same inputs go through the plain reference
-binary; results must agree to the tree's accuracy, with G applied and OldAcc
-set by the host code exactly as the reference's post-processing does.  After
-the start-up passes, both binaries also re-evaluate the system a drift later
-without rebuilding the tree: the reference drifts its nodes inside the walk
-(force_drift_node), the host code drifts the device tree (gg_drift).
+the two start-up gravity passes of compute_grav_accelerations) with the
+reference's own gravity/gravtree.c patched by oracle/patch_gravtree.py with
+the GRAVITY_GPU_B200 blocks that INTEGRATION.md documents: inside
+gravity_tree(), force_treebuild becomes gravtree_b200_build() and the walk /
+export loop becomes gravtree_b200_walk() (gizmo-public_b200/host/
+gravtree_b200.c, which hands GIZMO's own P[] records, strided, to the C ABI).
+Everything else is the reference's: move_particles and
+rearrange_particle_sequence before a build, and the post-processing that
+multiplies by G, sets OldAcc = |a|/G and switches to the relative criterion.
+The same inputs go through the plain reference binary; results must agree to
+the tree's accuracy.  After the start-up passes, both binaries also
+re-evaluate the system a drift later without rebuilding the tree: the
+reference drifts its nodes inside the walk (force_drift_node); the host code
+drifts the device tree's nodes (gg_drift) and hands it P[].Pos
+(gg_set_positions).
 """
 import numpy as np
 import pytest

@@ -62,3 +62,13 @@ def test_noalloc_sort_rejects_sizes_beyond_its_limit():
     v = torch.zeros(4, dtype=torch.int32, device="cuda")
     assert f(ggb200.NOALLOC_SORT_MAX_N + 1, k.data_ptr(), v.data_ptr(), 64, None) == -8   # GG_ERR_TOO_LARGE
     assert f(-1, k.data_ptr(), v.data_ptr(), 64, None) == -1
+
+
+def test_noalloc_sort_rejects_host_pointers():
+    """The pairs must be device memory of the current device, where the
+    static array is; host memory is refused before any kernel runs."""
+    f = _fn()
+    keys, vals = _pairs(1000, 7)
+    k0, v0 = keys.copy(), vals.copy()
+    assert f(1000, keys.ctypes.data, vals.ctypes.data, 64, None) == -1   # GG_ERR_INVALID
+    assert np.array_equal(keys, k0) and np.array_equal(vals, v0)
