@@ -21,8 +21,8 @@
 //     into chunks of leaf_size (the reference splits such near-coincident
 //     particles at random, forcetree.c:219-231).
 // Moments are FP64 sums (mass, mass-weighted position), children summed in
-// key order, with the centre of mass falling back to the geometric centre for
-// empty cells (forcetree.c:764-781).
+// key order, one depth per launch from the deepest up, with the centre of mass
+// falling back to the geometric centre for empty cells (forcetree.c:764-781).
 #include "gg_internal.cuh"
 #include "gg_kernels.cuh"
 
@@ -256,79 +256,71 @@ __global__ void __launch_bounds__(TB_THREADS) k_tree_write(int depth, const unsi
     }
 }
 
-// Bottom-up moments: each leaf sums its particles; the last child to finish
-// computes its parent (order-independent, children summed in index order).
-__global__ void k_tree_moments(const GGPart *__restrict__ parts, const GGDomainDev *__restrict__ dom, TreeBuf tb,
-                               GGNode *__restrict__ nodes)
+// Bottom-up moments, one depth per launch from the deepest up: a leaf sums its
+// particles, an internal node its children (one depth deeper, computed by the
+// previous launch), each in index order in FP64.  Nodes are numbered depth by
+// depth with the children of consecutive nodes consecutive, so the lanes of a
+// warp read one contiguous stretch of child records (or of particles).
+__global__ void k_tree_moments_depth(int depth, const GGPart *__restrict__ parts,
+                                     const GGDomainDev *__restrict__ dom, TreeBuf tb, GGNode *__restrict__ nodes)
 {
-    const int total = tb.nnodes[0];
-    for (int k0 = blockIdx.x * blockDim.x + threadIdx.x; k0 < total; k0 += gridDim.x * blockDim.x) {
-        if (tb.child[k0] >= 0) continue;   // only leaves start a climb
-        int k = k0;
-        bool is_leaf = true;
-        for (;;) {
-            const int lev = tb.level[k], sys = tb.sys[k];
-            const GGDomainDev d = dom[sys];
-            double M = 0, sx = 0, sy = 0, sz = 0;
-            float maxsoft = 0;
-            int a, b;
-            int s = tb.start[k];
-            if (is_leaf) {
-                int e = tb.end[k];
-                for (int i = s; i < e; i++) {
-                    GGPart p = parts[i];
-                    double m = (double)p.m;
-                    M += m;
-                    sx += m * p.x; sy += m * p.y; sz += m * p.z;
-                    maxsoft = fmaxf(maxsoft, p.h);
-                }
-                a = s;
-                b = -(e - s);
-            } else {
-                int c0 = tb.child[k], nc = tb.nch[k];
-                for (int c = c0; c < c0 + nc; c++) {
-                    double m = __ldcg(tb.mass64 + c);
-                    M += m;
-                    sx += m * __ldcg(&nodes[c].cx);
-                    sy += m * __ldcg(&nodes[c].cy);
-                    sz += m * __ldcg(&nodes[c].cz);
-                    maxsoft = fmaxf(maxsoft, __ldcg(&nodes[c].maxsoft));
-                }
-                a = c0;
-                b = nc;
+    const int lb = tb.depth_beg[depth], le = tb.depth_beg[depth + 1];
+    for (int k = lb + blockIdx.x * blockDim.x + threadIdx.x; k < le; k += gridDim.x * blockDim.x) {
+        const int lev = tb.level[k], sys = tb.sys[k];
+        const GGDomainDev d = dom[sys];
+        double M = 0, sx = 0, sy = 0, sz = 0;
+        float maxsoft = 0;
+        int a, b;
+        const int s = tb.start[k];
+        const int c0 = tb.child[k];
+        if (c0 < 0) {   // leaf: its particles
+            const int e = tb.end[k];
+            for (int i = s; i < e; i++) {
+                const GGPart p = parts[i];
+                const double m = (double)p.m;
+                M += m;
+                sx += m * p.x; sy += m * p.y; sz += m * p.z;
+                maxsoft = fmaxf(maxsoft, p.h);
             }
-            // geometric cell: level `lev` cell containing the node's first particle
-            int gl = lev > GG_MAX_LEVEL ? GG_MAX_LEVEL : lev;
-            double len = ldexp(d.len, -gl), cen[3];
-            if (gl == 0) {
-                cen[0] = d.center[0]; cen[1] = d.center[1]; cen[2] = d.center[2];
-            } else {
-                GGPart p0 = parts[s];
-                double pv[3] = {p0.x, p0.y, p0.z};
-                for (int q = 0; q < 3; q++) {
-                    unsigned cell = gg_quantize(pv[q], d.corner[q], d.len) >> (GG_MAX_LEVEL - gl);
-                    cen[q] = d.corner[q] + ((double)cell + 0.5) * len;
-                }
+            a = s;
+            b = -(e - s);
+        } else {        // internal: its children
+            const int nc = tb.nch[k];
+            for (int c = c0; c < c0 + nc; c++) {
+                const double m = tb.mass64[c];
+                M += m;
+                sx += m * nodes[c].cx;
+                sy += m * nodes[c].cy;
+                sz += m * nodes[c].cz;
+                maxsoft = fmaxf(maxsoft, nodes[c].maxsoft);
             }
-            double cx, cy, cz;
-            if (M > 0) { cx = sx / M; cy = sy / M; cz = sz / M; }
-            else { cx = cen[0]; cy = cen[1]; cz = cen[2]; }
-            GGNode nd;
-            nd.cx = cx; nd.cy = cy; nd.cz = cz;
-            nd.mass = (float)M; nd.len = (float)len; nd.maxsoft = maxsoft;
-            nd.gx = (float)(cen[0] - cx); nd.gy = (float)(cen[1] - cy); nd.gz = (float)(cen[2] - cz);
-            nd.a = a; nd.b = b; nd.level = lev; nd.parent = tb.parent[k];
-            nodes[k] = nd;
-            tb.mass64[k] = M;
-            int par = tb.parent[k];
-            if (par < 0) break;
-            __threadfence();
-            int old = atomicAdd(tb.counter + par, 1);
-            if (old != tb.nch[par] - 1) break;
-            __threadfence();
-            k = par;
-            is_leaf = false;
+            a = c0;
+            b = nc;
         }
+        // geometric cell: level `lev` cell containing the node's first particle
+        const int gl = lev > GG_MAX_LEVEL ? GG_MAX_LEVEL : lev;
+        const double len = ldexp(d.len, -gl);
+        double cen[3];
+        if (gl == 0) {
+            cen[0] = d.center[0]; cen[1] = d.center[1]; cen[2] = d.center[2];
+        } else {
+            const GGPart p0 = parts[s];
+            const double pv[3] = {p0.x, p0.y, p0.z};
+            for (int q = 0; q < 3; q++) {
+                const unsigned cell = gg_quantize(pv[q], d.corner[q], d.len) >> (GG_MAX_LEVEL - gl);
+                cen[q] = d.corner[q] + ((double)cell + 0.5) * len;
+            }
+        }
+        double cx, cy, cz;
+        if (M > 0) { cx = sx / M; cy = sy / M; cz = sz / M; }
+        else { cx = cen[0]; cy = cen[1]; cz = cen[2]; }
+        GGNode nd;
+        nd.cx = cx; nd.cy = cy; nd.cz = cz;
+        nd.mass = (float)M; nd.len = (float)len; nd.maxsoft = maxsoft;
+        nd.gx = (float)(cen[0] - cx); nd.gy = (float)(cen[1] - cy); nd.gz = (float)(cen[2] - cz);
+        nd.a = a; nd.b = b; nd.level = lev; nd.parent = tb.parent[k];
+        nodes[k] = nd;
+        tb.mass64[k] = M;
     }
 }
 
@@ -341,7 +333,9 @@ void gg_launch_permute(const unsigned *perm, const GGPart *in, GGPart *out, unsi
     gg_note_launches(1);
 }
 
-int gg_tree_grid() { return gg_num_sms() * 2; }
+// blocks of the per-depth count and write kernels: 8 per SM keeps enough binary
+// searches in flight to hide their dependent loads
+int gg_tree_grid() { return gg_num_sms() * 8; }
 
 void gg_launch_tree(const unsigned long long *keys, const int *poff, int S, int leaf, int cap, TreeBuf tb,
                     const GGPart *parts, const GGDomainDev *dom, GGNode *nodes, cudaStream_t st)
@@ -353,7 +347,8 @@ void gg_launch_tree(const unsigned long long *keys, const int *poff, int S, int 
         k_tree_scan<<<1, 1024, 0, st>>>(depth, tb, G, cap);
         k_tree_write<<<G, TB_THREADS, 0, st>>>(depth, keys, tb, leaf);
     }
-    int threads = 256, blocks = gg_num_sms() * 8;
-    k_tree_moments<<<blocks, threads, 0, st>>>(parts, dom, tb, nodes);
-    gg_note_launches(2 + 3 * GG_MAX_DEPTH);
+    const int threads = 256, blocks = gg_num_sms() * 8;
+    for (int depth = GG_MAX_DEPTH - 1; depth >= 0; depth--)
+        k_tree_moments_depth<<<blocks, threads, 0, st>>>(depth, parts, dom, tb, nodes);
+    gg_note_launches(1 + 4 * GG_MAX_DEPTH);
 }

@@ -26,8 +26,15 @@
 #ifndef GG_SORT_BITS
 #define GG_SORT_BITS 9
 #endif
+// 9-bit digits (7 passes for the 63-bit keys), 2048-key tiles, 4 blocks per
+// SM: measured best of {8,9} bits x {2048,3072,4096}-key tiles x 2-4 blocks per
+// SM on the 16.8M clustered system's keys (2.46 ms against 2.53 ms for 8-bit
+// digits; every variant within 12%: a pass is latency-bound, not tile-bound)
 #ifndef GG_SORT_ITEMS
-#define GG_SORT_ITEMS 16
+#define GG_SORT_ITEMS 8
+#endif
+#ifndef GG_SORT_MINB
+#define GG_SORT_MINB 4    // blocks per SM the pass kernel's registers must allow
 #endif
 #define SORT_THREADS 256
 #define SORT_ITEMS GG_SORT_ITEMS
@@ -142,7 +149,7 @@ struct SortSmem {
 // one pass: digit = (key >> shift) & (RADIX-1), or of the system id when sys_mode.
 // status: this pass's look-back words; status_next: the next pass's, of which
 // this tile clears its own (nullptr for the last pass)
-__global__ void __launch_bounds__(SORT_THREADS, 2) k_sort_pass(
+__global__ void __launch_bounds__(SORT_THREADS, GG_SORT_MINB) k_sort_pass(
     const unsigned long long *__restrict__ kin, const unsigned *__restrict__ vin, unsigned long long *__restrict__ kout,
     unsigned *__restrict__ vout, int n, int shift, int sys_mode, const int *__restrict__ poff, int S,
     const unsigned *__restrict__ g_off, unsigned *status, unsigned *status_next, unsigned *tile_counter, int *err)

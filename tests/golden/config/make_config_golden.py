@@ -58,9 +58,12 @@ CASES = {
     "galaxy_262144_tol0025": (0.0025, 4096, 11, 0.0),
     "galaxy_262144_tol005": (0.005, 4096, 11, 0.0),
     "galaxy_4194304_tol001": (0.001, 4096, 12, 0.0),
+    "galaxy_4194304_tol0025": (0.0025, 4096, 12, 0.0),
+    "galaxy_4194304_tol005": (0.005, 4096, 12, 0.0),
     "clustered_1048576_tol0025": (0.0025, 4096, 13, 0.1),
     "clustered_1048576_tol0008": (0.0008, 4096, 13, 0.1),
     "clustered_16777216_tol0008": (0.0008, 2048, 14, 0.1),
+    "clustered_16777216_tol0025": (0.0025, 2048, 14, 0.1),
 }
 ACTIVE_SEED = 77
 
