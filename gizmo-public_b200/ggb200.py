@@ -50,7 +50,7 @@ class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("leaf_size", ctypes.c_int32), ("group_size", ctypes.c_int32),
                 ("flush_threshold", ctypes.c_int32), ("walk_blocks_per_sm", ctypes.c_int32),
                 ("timing", ctypes.c_int32), ("target_order", ctypes.c_int32), ("group_order", ctypes.c_int32),
-                ("node_staging", ctypes.c_int32)]
+                ("node_staging", ctypes.c_int32), ("walk_stack_entries", ctypes.c_int32)]
 
 
 class Domain(ctypes.Structure):
@@ -178,7 +178,7 @@ class GravityTree:
     """One library context: particles of one or more systems, their trees, walks."""
 
     def __init__(self, leaf_size=8, group_size=32, flush=128, device=0, timing=False, blocks_per_sm=0, target_order=1,
-                 group_order=1, node_staging=0):
+                 group_order=1, node_staging=0, walk_stack_entries=0):
         lib = load_library()
         cfg = Config()
         lib.gg_config_default(ctypes.byref(cfg))
@@ -188,6 +188,7 @@ class GravityTree:
         cfg.target_order = target_order
         cfg.group_order = group_order
         cfg.node_staging = node_staging
+        cfg.walk_stack_entries = walk_stack_entries
         h = ctypes.c_void_p()
         _check(lib.gg_create(ctypes.byref(cfg), ctypes.byref(h)), "gg_create")
         self._lib, self._h = lib, h

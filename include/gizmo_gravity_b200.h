@@ -70,6 +70,14 @@ typedef struct gg_config {
                                  completing on an mbarrier (force walks of groups > 1; the
                                  exact and potential-only walks stage per lane).  Same results;
                                  gg_autotune tries both */
+    int32_t walk_stack_entries; /* entries of each walk warp's node stack in device memory
+                                 beyond its 512 in shared memory, 0 = default (8192).  A
+                                 blocking evaluation whose stack overflows is run again with
+                                 four times the entries (up to 131072), from the same OldAcc,
+                                 as the reference grows its node pool and rebuilds
+                                 (forcetree.c:112-125), and a step captured by
+                                 gg_graph_capture_step must then be captured again; an
+                                 asynchronous evaluation reports GG_ERR_OVERFLOW */
 } gg_config;
 
 /* root cube of one system: domain_findExtent (domain.c:2518-2570) */
@@ -260,12 +268,13 @@ gg_status gg_graph_launch(gg_ctx *ctx);
  * *chosen and its walk time in *best_ms (nullable).  The gate: on a fixed
  * sample of targets (every target of a system of up to 2,048 particles, else
  * 16,384 / n_systems evenly spaced ones, at least 64 and at most 4,096)
- * against their FP64 direct sums, a candidate's
- * 99th-percentile relative force error must be at most 1.1x the context's own
- * configuration's in every system (plus 1e-7), and its sample potential energy
- * 1/2 sum m phi no further from the direct sum's than 1.1x the context's own,
- * or within 1e-5 relative; so a faster configuration is never taken at the
- * price of accuracy.  No counterpart in the reference.  Synchronises. */
+ * against their FP64 direct sums, a candidate's 99th-percentile relative force
+ * error over all sampled targets, and the largest of the systems' own 99th
+ * percentiles, must each be at most 1.1x the context's own configuration's
+ * (plus 1e-7), and the root mean square over systems of the sample potential
+ * energy's (1/2 sum m phi) relative error at most 1.1x the context's own or
+ * below 1e-5; so a faster configuration is never taken at the price of
+ * accuracy.  No counterpart in the reference.  Synchronises. */
 gg_status gg_autotune(gg_ctx *ctx, double err_tol_force_acc, double err_tol_theta, gg_config *chosen,
                       double *best_ms);
 /* The same search for the walk of an active subset (device indices in load

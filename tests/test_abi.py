@@ -47,7 +47,8 @@ def test_invalid_arguments_rejected_without_device():
     lib = ggb200.load_library()
     cfg = ggb200.Config()
     lib.gg_config_default(ctypes.byref(cfg))
-    assert cfg.group_order == 1 and cfg.target_order == 1 and cfg.node_staging == 0 and ctypes.sizeof(cfg) == 36
+    assert cfg.group_order == 1 and cfg.target_order == 1 and cfg.node_staging == 0 and ctypes.sizeof(cfg) == 40
+    assert cfg.walk_stack_entries == 0
     cfg.leaf_size = 0
     h = ctypes.c_void_p()
     assert lib.gg_create(ctypes.byref(cfg), ctypes.byref(h)) == -1
@@ -56,6 +57,9 @@ def test_invalid_arguments_rejected_without_device():
     assert lib.gg_create(ctypes.byref(cfg), ctypes.byref(h)) == -1
     lib.gg_config_default(ctypes.byref(cfg))
     cfg.node_staging = 2
+    assert lib.gg_create(ctypes.byref(cfg), ctypes.byref(h)) == -1
+    lib.gg_config_default(ctypes.byref(cfg))
+    cfg.walk_stack_entries = -1
     assert lib.gg_create(ctypes.byref(cfg), ctypes.byref(h)) == -1
     assert lib.gg_radix_sort_pairs(-1, None, None, 64, None) == -1
 

@@ -256,3 +256,35 @@ def test_bounded_wait_returns_timeout_and_the_device_stays_usable():
     ggb200.radix_sort_pairs(dk, dv, 10000, 64)
     torch.cuda.synchronize()
     assert np.array_equal(dk.cpu().numpy().view(np.uint64), np.sort(keys))
+
+
+def test_walk_stack_overflow_is_retried_with_a_larger_stack():
+    """A node stack far too small for the walk (64 device entries per warp
+    beyond the 512 in shared memory) and a walk that opens every node (the
+    relative criterion with OldAcc 0): the asynchronous form reports the
+    overflow; the blocking evaluation runs again with a larger stack, from the
+    same OldAcc, as the reference grows its node pool and rebuilds, and gives
+    the bits of a default run."""
+    import torch
+    ic = ics.plummer(40000, seed=33)
+    n = ic["pos"].shape[0]
+    zero = np.zeros(n)
+    with ggb200.GravityTree(walk_stack_entries=64) as t:
+        t.load(ic["pos"], ic["mass"], ic["h"])
+        t.build()
+        d = torch.empty((n, 3), dtype=torch.float64, device="cuda")
+        t.evaluate_device(d, None, d_old_acc=torch.zeros(n, dtype=torch.float64, device="cuda"),
+                          err_tol_force_acc=0.001, err_tol_theta=0.0)
+        with pytest.raises(ggb200.GravityError) as ei:
+            t.last_stats()
+        assert ei.value.status == -4   # GG_ERR_OVERFLOW
+    res = []
+    for entries in (0, 64):
+        with ggb200.GravityTree(walk_stack_entries=entries) as t:
+            t.load(ic["pos"], ic["mass"], ic["h"])
+            t.build()
+            res.append(t.evaluate(old_acc=zero, err_tol_force_acc=0.001, want_ninter=True))
+            res.append(t.evaluate(old_acc=np.linalg.norm(res[-1][0], axis=1), err_tol_force_acc=0.001))
+    assert res[1][3]["error_word"] == 0 and res[3][3]["error_word"] == 0
+    assert np.array_equal(res[0][0], res[2][0]) and np.array_equal(res[0][2], res[2][2])
+    assert np.array_equal(res[1][0], res[3][0])
