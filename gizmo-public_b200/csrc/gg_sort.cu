@@ -38,12 +38,7 @@
 #ifndef GG_SORT_MINB
 #define GG_SORT_MINB 4    // blocks per SM the pass kernel's registers must allow
 #endif
-#ifndef GG_SORT_SEG
-#define GG_SORT_SEG 1     // passes in the reduce-then-scan form (0: one-sweep with look-back)
-#endif
-#ifndef GG_SORT_SEGS_PER_SM
-#define GG_SORT_SEGS_PER_SM 8
-#endif
+
 #define SORT_THREADS 256
 #define SORT_ITEMS GG_SORT_ITEMS
 #define SORT_TILE (SORT_THREADS * SORT_ITEMS)
@@ -154,43 +149,22 @@ struct SortSmem {
     int tile;
 };
 
-// One pass: digit = (key >> shift) & (RADIX-1), or of the system id when
-// sys_mode.  Two forms of the same tile work:
-//   SEG = false (one-sweep): a CTA takes one tile from tile_counter and finds
-//     where its digits start by a decoupled look-back over its predecessors'
-//     status words (status: this pass's; status_next: the next pass's, of
-//     which this tile clears its own, nullptr for the last pass);
-//   SEG = true (reduce-then-scan): CTA s owns the tiles [s*tps, (s+1)*tps)
-//     and walks them in order; where its digits start comes from seg_off
-//     (the exclusive scan over segments of the per-segment digit counts,
-//     digit-major: seg_off[d * nseg + s]), advanced by each tile's counts.
-//     No CTA waits on another.
-template <bool SEG>
+// one pass: digit = (key >> shift) & (RADIX-1), or of the system id when sys_mode.
+// status: this pass's look-back words; status_next: the next pass's, of which
+// this tile clears its own (nullptr for the last pass)
 __global__ void __launch_bounds__(SORT_THREADS, GG_SORT_MINB) k_sort_pass(
     const unsigned long long *__restrict__ kin, const unsigned *__restrict__ vin, unsigned long long *__restrict__ kout,
     unsigned *__restrict__ vout, int n, int shift, int sys_mode, const int *__restrict__ poff, int S,
-    const unsigned *__restrict__ g_off, unsigned *status, unsigned *status_next, unsigned *tile_counter, int *err,
-    int tps, int nseg, const unsigned *__restrict__ seg_off)
+    const unsigned *__restrict__ g_off, unsigned *status, unsigned *status_next, unsigned *tile_counter, int *err)
 {
     extern __shared__ __align__(16) unsigned char sort_smem_raw[];
     SortSmem &sm = *reinterpret_cast<SortSmem *>(sort_smem_raw);
 
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const long long ntiles_all = ((long long)n + SORT_TILE - 1) / SORT_TILE;
-    int tile_first = 0, tile_end = 0;
-    unsigned running[DPT];   // SEG: where this CTA's next tile puts each of its thread's digits
-    if (SEG) {
-        tile_first = blockIdx.x * tps;
-        tile_end = (int)min((long long)tile_first + tps, ntiles_all);
-#pragma unroll
-        for (int q = 0; q < DPT; q++) running[q] = seg_off[(size_t)(DPT * tid + q) * nseg + blockIdx.x];
-    } else {
-        if (tid == 0) sm.tile = (int)atomicAdd(tile_counter, 1u);
-    }
-    for (int tile_it = tile_first; SEG ? tile_it < tile_end : tile_it == 0; tile_it++) {
+    if (tid == 0) sm.tile = (int)atomicAdd(tile_counter, 1u);
     for (int i = tid; i < SORT_WARPS * RADIX; i += SORT_THREADS) (&sm.whist[0][0])[i] = 0;
     __syncthreads();
-    const int tile = SEG ? tile_it : sm.tile;
+    const int tile = sm.tile;
     const long long tile_base = (long long)tile * SORT_TILE;
     const long long wbase = tile_base + (long long)w * 32 * SORT_ITEMS;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -241,17 +215,10 @@ __global__ void __launch_bounds__(SORT_THREADS, GG_SORT_MINB) k_sort_pass(
         }
         sum[q] = acc;
     }
-    if (SEG) {   // where this tile's digits start: the segment's running offsets
-#pragma unroll
-        for (int q = 0; q < DPT; q++) {
-            sm.gbase[DPT * tid + q] = running[q];
-            running[q] += sum[q];
-        }
-    }
     // publish and look back, digit by digit
     unsigned *st = status + (size_t)tile * RADIX;
 #pragma unroll
-    for (int q = 0; q < DPT && !SEG; q++) {
+    for (int q = 0; q < DPT; q++) {
         const int d = DPT * tid + q;
         unsigned excl = 0;
         if (tile == 0) {
@@ -312,67 +279,6 @@ __global__ void __launch_bounds__(SORT_THREADS, GG_SORT_MINB) k_sort_pass(
             vout[gpos] = sm.vals[i];
         }
     }
-    __syncthreads();   // the next tile reuses the shared buffers
-    }
-}
-
-// reduce-then-scan, step 1: each segment's digit counts, digit-major
-// (counts[d * nseg + s]); per-warp histograms in shared memory
-__global__ void __launch_bounds__(SORT_THREADS) k_sort_seg_count(const unsigned long long *__restrict__ kin,
-                                                                const unsigned *__restrict__ vin, int n, int shift,
-                                                                int sys_mode, const int *__restrict__ poff, int S,
-                                                                int tps, int nseg, unsigned *__restrict__ counts)
-{
-    __shared__ unsigned h[SORT_WARPS][RADIX];
-    const int tid = threadIdx.x, w = tid >> 5;
-    for (int i = tid; i < SORT_WARPS * RADIX; i += SORT_THREADS) (&h[0][0])[i] = 0;
-    __syncthreads();
-    const long long b = (long long)blockIdx.x * tps * SORT_TILE;
-    const long long e = min((long long)n, b + (long long)tps * SORT_TILE);
-    for (long long i = b + tid; i < e; i += SORT_THREADS) {
-        const unsigned d = sys_mode ? ((unsigned)sort_sys_of(poff, S, vin[i]) >> shift) & (RADIX - 1)
-                                    : (unsigned)(kin[i] >> shift) & (RADIX - 1);
-        atomicAdd(&h[w][d], 1u);
-    }
-    __syncthreads();
-    for (int d = tid; d < RADIX; d += SORT_THREADS) {
-        unsigned t = 0;
-#pragma unroll
-        for (int ww = 0; ww < SORT_WARPS; ww++) t += h[ww][d];
-        counts[(size_t)d * nseg + blockIdx.x] = t;
-    }
-}
-
-// reduce-then-scan, step 2: one block per digit scans its segments' counts
-// (exclusive) from the digit's global offset
-__global__ void __launch_bounds__(SORT_THREADS) k_sort_seg_scan(const unsigned *__restrict__ counts, int nseg,
-                                                               const unsigned *__restrict__ g_off,
-                                                               unsigned *__restrict__ seg_off)
-{
-    __shared__ unsigned s_wsum[SORT_WARPS];
-    __shared__ unsigned s_carry;
-    const int d = blockIdx.x, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    if (tid == 0) s_carry = g_off[d];
-    __syncthreads();
-    for (int base = 0; base < nseg; base += SORT_THREADS) {
-        const int s = base + tid;
-        const unsigned v = s < nseg ? counts[(size_t)d * nseg + s] : 0u;
-        unsigned x = v;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane == 31) s_wsum[w] = x;
-        __syncthreads();
-        unsigned wo = 0;
-        for (int ww = 0; ww < w; ww++) wo += s_wsum[ww];
-        const unsigned carry = s_carry;
-        if (s < nseg) seg_off[(size_t)d * nseg + s] = carry + wo + x - v;
-        __syncthreads();
-        if (tid == SORT_THREADS - 1) s_carry = carry + wo + x;
-        __syncthreads();
-    }
 }
 
 static int sort_passes(int bits) { return bits <= 0 ? 0 : (bits + SORT_BITS - 1) / SORT_BITS; }
@@ -418,17 +324,9 @@ gg_status gg_sort_pairs_run(unsigned long long *keys, unsigned *vals, long long 
     unsigned *counters = (unsigned *)take(256);
     unsigned *status[2] = {(unsigned *)take((size_t)ntiles * RADIX * 4), (unsigned *)take((size_t)ntiles * RADIX * 4)};
 
-    // reduce-then-scan: segments of tps consecutive tiles, about GG_SORT_SEGS_PER_SM per SM;
-    // their digit counts and scanned offsets use the status arrays' space
-    const bool seg = GG_SORT_SEG != 0;
-    long long nseg = std::min<long long>(ntiles, (long long)gg_num_sms() * GG_SORT_SEGS_PER_SM);
-    const int tps = (int)((ntiles + nseg - 1) / nseg);
-    nseg = (ntiles + tps - 1) / tps;
     GG_CUDA_TRY(cudaMemsetAsync(hist, 0, (size_t)np * RADIX * 4, st));
-    if (!seg) {
-        GG_CUDA_TRY(cudaMemsetAsync(counters, 0, 256, st));
-        GG_CUDA_TRY(cudaMemsetAsync(status[0], 0, (size_t)ntiles * RADIX * 4, st));
-    }
+    GG_CUDA_TRY(cudaMemsetAsync(counters, 0, 256, st));
+    GG_CUDA_TRY(cudaMemsetAsync(status[0], 0, (size_t)ntiles * RADIX * 4, st));
     {
         int threads = 256, blocks = gg_num_sms() * 4;
         const long long need = (n + threads - 1) / threads;
@@ -440,29 +338,16 @@ gg_status gg_sort_pairs_run(unsigned long long *keys, unsigned *vals, long long 
         gg_note_launches(2);
     }
     // the attribute is per device: set it on every call (cheap)
-    GG_CUDA_TRY(cudaFuncSetAttribute(k_sort_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     sort_smem_bytes()));
-    GG_CUDA_TRY(cudaFuncSetAttribute(k_sort_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     sort_smem_bytes()));
+    GG_CUDA_TRY(cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, sort_smem_bytes()));
     unsigned long long *ka = keys, *kb = kalt;
     unsigned *va = vals, *vb = valt;
     for (int pass = 0; pass < np; pass++) {
         const int sys_mode = pass >= nkey;
         const int shift = sys_mode ? SORT_BITS * (pass - nkey) : SORT_BITS * pass;
-        if (seg) {
-            k_sort_seg_count<<<(unsigned)nseg, SORT_THREADS, 0, st>>>(ka, va, (int)n, shift, sys_mode, poff, S, tps,
-                                                                     (int)nseg, status[0]);
-            k_sort_seg_scan<<<RADIX, SORT_THREADS, 0, st>>>(status[0], (int)nseg, off + pass * RADIX, status[1]);
-            k_sort_pass<true><<<(unsigned)nseg, SORT_THREADS, sort_smem_bytes(), st>>>(
-                ka, va, kb, vb, (int)n, shift, sys_mode, poff, S, off + pass * RADIX, nullptr, nullptr, nullptr, err,
-                tps, (int)nseg, status[1]);
-            gg_note_launches(3);
-        } else {
-            k_sort_pass<false><<<(unsigned)ntiles, SORT_THREADS, sort_smem_bytes(), st>>>(
-                ka, va, kb, vb, (int)n, shift, sys_mode, poff, S, off + pass * RADIX, status[pass & 1],
-                pass + 1 < np ? status[(pass + 1) & 1] : nullptr, counters + pass, err, 0, 0, nullptr);
-            gg_note_launches(1);
-        }
+        k_sort_pass<<<(unsigned)ntiles, SORT_THREADS, sort_smem_bytes(), st>>>(
+            ka, va, kb, vb, (int)n, shift, sys_mode, poff, S, off + pass * RADIX, status[pass & 1],
+            pass + 1 < np ? status[(pass + 1) & 1] : nullptr, counters + pass, err);
+        gg_note_launches(1);
         unsigned long long *tk = ka; ka = kb; kb = tk;
         unsigned *tv = va; va = vb; vb = tv;
     }
@@ -498,9 +383,9 @@ gg_status gg_sort_timeout_selftest(cudaStream_t st)
     cudaMemsetAsync(base, 0, (size_t)(p - base), st);
     const unsigned one = 1;   // the CTA takes tile 1; tile 0 is never started
     cudaMemcpyAsync(counter, &one, sizeof one, cudaMemcpyHostToDevice, st);
-    cudaFuncSetAttribute(k_sort_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sort_smem_bytes());
-    k_sort_pass<false><<<1, SORT_THREADS, sort_smem_bytes(), st>>>(kin, vin, kout, vout, n, 0, 0, nullptr, 1, off,
-                                                                    status, nullptr, counter, err, 0, 0, nullptr);
+    cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, sort_smem_bytes());
+    k_sort_pass<<<1, SORT_THREADS, sort_smem_bytes(), st>>>(kin, vin, kout, vout, n, 0, 0, nullptr, 1, off, status,
+                                                             nullptr, counter, err);
     gg_note_launches(1);
     int herr = 0;
     cudaError_t e = cudaGetLastError();

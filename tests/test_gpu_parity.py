@@ -30,7 +30,7 @@ def test_keys_bitwise_equal_oracle():
     assert np.array_equal(got, lo)
 
 
-@pytest.mark.parametrize("n", [2, 3, 4095, 4096, 4097, 100003, 1 << 20, 5000011])
+@pytest.mark.parametrize("n", [2, 3, 4095, 4096, 4097, 100003, 1 << 20, 5000011, 1 << 24])
 def test_radix_sort_is_stable_and_exact(n):
     torch = torch_cuda()
     rng = np.random.default_rng(n)
