@@ -199,6 +199,11 @@ struct gg_ctx {
     DevBuf<unsigned long long> extent_mm;
     DevBuf<unsigned> hmm;          // per system [min h, max h] as float bits
     bool h_mixed = false;          // some system holds several kernel radii: group targets by softening
+    // gg_load_particles_device: the per-system kernel-radius range crosses to
+    // pinned memory behind the extent pass; the first walk reads it (hmm_ev)
+    bool h_mixed_pending = false;
+    HostBuf<unsigned> h_hmm;
+    cudaEvent_t hmm_ev = nullptr;
     int order_by_softening = 1;    // from gg_config.target_order
     DevBuf<unsigned long long> tkey;
     DevBuf<unsigned> tval;
@@ -238,6 +243,7 @@ struct gg_ctx {
     DevBuf<unsigned> gorder;
     DevBuf<GGGroup> groups;
     DevBuf<int> ngroups, gscan, toff, flag, flagscan, tlist, tout, scan_scratch, active_d;
+    DevBuf<int> g_node, g_flag, g_seg, g_segstart;   // group building scratch
     DevBuf<int> counters;                  // [0] group counter
     DevBuf<unsigned long long> inter;      // interaction total
     DevBuf<int> stack;
@@ -288,6 +294,7 @@ struct gg_ctx {
         f(oldacc); f(vel); f(newpos); f(kin); f(kin_counter); f(dts); f(oldacc_save); f(tcost); f(gkey); f(gorder);
         f(e_chunks); f(e_first); f(e_part); f(e_out);
         f(groups); f(ngroups); f(gscan); f(toff); f(flag); f(flagscan); f(tlist); f(tout); f(scan_scratch);
+        f(g_node); f(g_flag); f(g_seg); f(g_segstart);
         f(active_d); f(counters); f(inter); f(stack); f(err); f(acc_d); f(pot_d); f(nint_d); f(oldacc_in);
         f(tune_tg); f(tune_rows); f(tune_acc); f(tune_pot); f(tune_mass); f(tune_gacc); f(tune_gpot);
     }
@@ -392,6 +399,7 @@ extern "C" gg_status gg_create(const gg_config *cfg, gg_ctx **out)
         (e = cudaEventCreateWithFlags(&ctx->done_ev, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&ctx->old_ready_ev, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&ctx->old_used_ev, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->hmm_ev, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking)) != cudaSuccess) {
         gg_destroy(ctx);
         return gg_cuda_fail(e);
@@ -428,7 +436,9 @@ extern "C" gg_status gg_destroy(gg_ctx *c)
     c->h_nint.give_back(c->done_ev);
     c->h_vstage.give_back(c->vstage_ev);
     c->h_stage.give_back(c->stage_ev);
+    c->h_hmm.give_back(c->hmm_ev);
     if (c->act_ev) cudaEventDestroy(c->act_ev);
+    if (c->hmm_ev) cudaEventDestroy(c->hmm_ev);
     for (int i = 0; i < kPipeEvents; i++)
         if (c->pipe_ev[i]) cudaEventDestroy(c->pipe_ev[i]);
     if (c->done_ev) cudaEventDestroy(c->done_ev);
@@ -530,6 +540,7 @@ extern "C" gg_status gg_load_particles(gg_ctx *c, int32_t S, const int64_t *coun
     // a change of kernel radius between neighbouring particles of different
     // systems also counts: harmless (ordering then just keeps each system's order)
     c->h_mixed = mixed != 0;
+    c->h_mixed_pending = false;
     GG_CUDA_TRY(cudaEventRecord(c->stage_ev, c->stream));
     return GG_OK;
 }
@@ -542,15 +553,28 @@ extern "C" gg_status gg_load_particles_device(gg_ctx *c, int32_t S, const int64_
     if ((st = set_systems(c, S, counts))) return st;
     if (c->N) {
         GG_CUDA_TRY(cudaMemcpyAsync(c->in_rec.p, d_records, c->N * sizeof(GGPart), cudaMemcpyDeviceToDevice, c->stream));
-        // the range of kernel radii decides (once, here) whether walks order targets by softening
+        // the range of kernel radii decides whether walks order targets by
+        // softening; it crosses to pinned memory behind the extent pass and the
+        // first walk reads it, so the load does not wait for the device
         gg_launch_extent(c->in_rec.p, (int)c->N, c->poff.p, S, c->extent_mm.p, c->hmm.p, c->dom.p, c->err.p, c->stream);
-        std::vector<unsigned> h(2 * (size_t)S);
-        GG_CUDA_TRY(cudaMemcpyAsync(h.data(), c->hmm.p, h.size() * sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
-        GG_CUDA_TRY(cudaStreamSynchronize(c->stream));
-        c->h_mixed = false;
-        for (int s = 0; s < S; s++)
-            if (h[2 * s] != h[2 * s + 1] && h[2 * s] != 0x7f800000u) c->h_mixed = true;
+        if ((st = c->h_hmm.ensure(2 * (size_t)S, c->hmm_ev))) return st;
+        GG_CUDA_TRY(cudaMemcpyAsync(c->h_hmm.p, c->hmm.p, 2 * (size_t)S * sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                    c->stream));
+        GG_CUDA_TRY(cudaEventRecord(c->hmm_ev, c->stream));
+        c->h_mixed_pending = true;
     }
+    return GG_OK;
+}
+
+// the kernel-radius ranges of a device load, once they have reached the host
+static gg_status resolve_h_mixed(gg_ctx *c)
+{
+    if (!c->h_mixed_pending) return GG_OK;
+    GG_CUDA_TRY(cudaEventSynchronize(c->hmm_ev));
+    c->h_mixed = false;
+    for (int s = 0; s < c->S; s++)
+        if (c->h_hmm.p[2 * s] != c->h_hmm.p[2 * s + 1] && c->h_hmm.p[2 * s] != 0x7f800000u) c->h_mixed = true;
+    c->h_mixed_pending = false;
     return GG_OK;
 }
 
@@ -659,9 +683,12 @@ static gg_status walk_setup(gg_ctx *c)
         if (per_sm > 3) per_sm = 3;
         c->walk_blocks = per_sm;   // blocks per SM; the grid is that many per SM
     }
-    long long maxg = c->N / c->cfg.group_size + c->S + 1;
+    const long long maxg = gg_max_groups(c->N, c->S, c->cfg.group_size);
     if ((st = c->groups.ensure(maxg)) || (st = c->ngroups.ensure(2)) || (st = c->gscan.ensure(c->S + 1)) ||
         (st = c->toff.ensure(c->S + 1)) ||
+        (c->cfg.group_size > 1 &&
+         ((st = c->g_node.ensure(c->N + 1)) || (st = c->g_flag.ensure(c->N + 1)) || (st = c->g_seg.ensure(c->N + 1)) ||
+          (st = c->g_segstart.ensure(c->N + 1)))) ||
         (st = c->stack.ensure((size_t)c->walk_blocks * gg_num_sms() * (gg_walk_threads() / 32) * c->stack_cap)) ||
         (st = c->scan_scratch.ensure(gg_scan_scratch_ints())))
         return st;
@@ -680,6 +707,7 @@ static gg_status run_walk(gg_ctx *c, const int *d_active, int n_active, const do
     gg_status st;
     cudaStream_t s = c->stream;
     if ((st = walk_setup(c))) return st;
+    if ((st = resolve_h_mixed(c))) return st;
     const int S = c->S, N = (int)c->N;
     const int *tlist = nullptr, *tout = nullptr;
     const int *toff = c->poff.p;
@@ -709,12 +737,20 @@ static gg_status run_walk(gg_ctx *c, const int *d_active, int n_active, const do
         GG_CUDA_TRY(cudaMemcpyAsync(c->oldacc.p, d_old_acc, (size_t)N * sizeof(double), cudaMemcpyDeviceToDevice, s));
         c->oldacc_valid = true;
     }
-    gg_launch_groups(toff, S, c->cfg.group_size, c->groups.p, c->ngroups.p, c->gscan.p, s);
+    const long long maxg = gg_max_groups(c->N, c->S, c->cfg.group_size);
+    if (c->cfg.group_size > 1) {
+        const bool by_soft = c->h_mixed && c->order_by_softening;
+        gg_launch_groups_tree(d_active ? n_active : N, tlist, d_active ? c->flagscan.p : nullptr, toff, S,
+                              c->cfg.group_size, tree_buf(c), by_soft ? c->dom.p : nullptr, c->hmm.p,
+                              gg_target_order_lmax(S), c->g_node.p, c->g_flag.p, c->g_seg.p, c->g_segstart.p,
+                              (int)maxg, c->groups.p, c->ngroups.p, c->scan_scratch.p, c->err.p, s);
+    } else {
+        gg_launch_groups(toff, S, c->cfg.group_size, c->groups.p, c->ngroups.p, c->gscan.p, s);
+    }
     const unsigned *gorder = nullptr;
     if (c->cfg.group_order && !c->tcost_valid)   // a fresh history: targets not walked yet cost 0
         GG_CUDA_TRY(cudaMemsetAsync(c->tcost.p, 0, (size_t)c->N * sizeof(float), s));
     if (c->cfg.group_order && c->tcost_valid) {
-        const long long maxg = c->N / c->cfg.group_size + c->S + 1;
         if ((st = gg_order_groups_by_cost(c->groups.p, c->ngroups.p, (int)maxg, tlist, c->perm.p, c->tcost.p,
                                           c->gkey.p, c->gorder.p, c->sort_scratch.p, c->err.p, s)))
             return st;
@@ -1013,8 +1049,9 @@ extern "C" gg_status gg_graph_capture_step(gg_ctx *c, double tol, double theta, 
     if ((st = set_device(c))) return st;
     if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
     if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
-    // grow every buffer the walk may need before capturing
+    // grow every buffer the walk may need, and read the kernel-radius ranges, before capturing
     if ((st = walk_setup(c))) return st;
+    if ((st = resolve_h_mixed(c))) return st;
     const int timing = c->cfg.timing;
     c->cfg.timing = 0;
     long long before = gg_kernel_launches();
@@ -1545,6 +1582,7 @@ extern "C" gg_status gg_load_systems(gg_ctx *c, int32_t S, const int64_t *counts
         }
     }
     c->h_mixed = mixed != 0;
+    c->h_mixed_pending = false;
     if (c->N) GG_CUDA_TRY(cudaMemcpyAsync(c->in_rec.p, c->h_stage.p, c->N * sizeof(GGPart), cudaMemcpyHostToDevice,
                                           c->stream));
     GG_CUDA_TRY(cudaEventRecord(c->stage_ev, c->stream));

@@ -64,6 +64,12 @@ int gg_walk_threads();
 
 // groups of `gs` consecutive targets per system; toff[S+1] target offsets per system
 void gg_launch_groups(const int *toff, int S, int gs, GGGroup *groups, int *ngroups, int *gscan, cudaStream_t st);
+long long gg_max_groups(long long n, int S, int gs);
+int gg_target_order_lmax(int S);
+void gg_launch_groups_tree(int nt, const int *tlist, const int *tscan, const int *toff, int S, int gs,
+                           const TreeBuf &tb, const GGDomainDev *order_dom, const unsigned *hmm, int lmax, int *gnode,
+                           int *flag, int *seg, int *segstart, int maxg, GGGroup *groups, int *ngroups,
+                           int *scan_scratch, int *err, cudaStream_t st);
 // exclusive scan of n ints (scratch: 2 * (gg_num_sms()*4) ints)
 void gg_launch_scan(const int *in, int *out, int n, int *scratch, cudaStream_t st);
 // active targets: flags in sorted order -> tlist/tout, and per-system offsets

@@ -1,13 +1,15 @@
 // gg_util.cu -- scans, walk-group tables, active-target compaction and the
 // FP64 direct summation used to measure force errors.
 #include <algorithm>
+#include <climits>
 
 #include "gg_internal.cuh"
 #include "gg_kernels.cuh"
 
 #define SC_THREADS 256
+#define SC_ITEMS 8   // consecutive elements per thread: one block-wide scan per 2048
 
-static int scan_blocks() { return gg_num_sms() * 2; }
+static int scan_blocks() { return gg_num_sms() * 4; }
 int gg_scan_scratch_ints() { return scan_blocks() + 64; }
 
 // ---- exclusive scan of n ints into out[0..n] (out[n] = total); in may be
@@ -44,8 +46,13 @@ __global__ void k_scan_reduce(const int *__restrict__ in, int n, int nonzero, in
     const int G = gridDim.x, chunk = (n + G - 1) / G;
     const int cb = blockIdx.x * chunk, ce = min(n, cb + chunk);
     int acc = 0;
-    for (int i = cb + threadIdx.x; i < ce; i += blockDim.x) {
-        int v = in[i];
+    int i = cb + threadIdx.x;
+    for (; i + 3 * SC_THREADS < ce; i += 4 * SC_THREADS) {   // four loads in flight per thread
+        const int a = in[i], b = in[i + SC_THREADS], c = in[i + 2 * SC_THREADS], d = in[i + 3 * SC_THREADS];
+        acc += nonzero ? (a != 0) + (b != 0) + (c != 0) + (d != 0) : a + b + c + d;
+    }
+    for (; i < ce; i += SC_THREADS) {
+        const int v = in[i];
         acc += nonzero ? (v != 0) : v;
     }
     int tot;
@@ -67,19 +74,31 @@ __global__ void k_scan_top(int *bsum, int G)
     if (threadIdx.x == 0) bsum[G] = carry;
 }
 
+// each thread scans SC_ITEMS consecutive elements of a 2048-element tile in
+// registers; one block-wide scan of the threads' sums per tile
 __global__ void k_scan_down(const int *__restrict__ in, int n, int nonzero, const int *__restrict__ bsum, int *out)
 {
     __shared__ int ws[33];
     const int G = gridDim.x, chunk = (n + G - 1) / G;
     const int cb = blockIdx.x * chunk, ce = min(n, cb + chunk);
     int run = bsum[blockIdx.x];
-    for (int base = cb; base < ce; base += blockDim.x) {
-        int i = base + threadIdx.x;
-        int v = 0;
-        if (i < ce) { v = in[i]; if (nonzero) v = (v != 0); }
+    for (int base = cb; base < ce; base += SC_THREADS * SC_ITEMS) {
+        const int i0 = base + threadIdx.x * SC_ITEMS;
+        int v[SC_ITEMS], sum = 0;
+#pragma unroll
+        for (int j = 0; j < SC_ITEMS; j++) {
+            int x = i0 + j < ce ? in[i0 + j] : 0;
+            if (nonzero) x = (x != 0);
+            v[j] = x;
+            sum += x;
+        }
         int tot;
-        int e = block_excl_scan(v, ws, &tot);
-        if (i < ce) out[i] = run + e;
+        int r = run + block_excl_scan(sum, ws, &tot);
+#pragma unroll
+        for (int j = 0; j < SC_ITEMS; j++) {
+            if (i0 + j < ce) out[i0 + j] = r;
+            r += v[j];
+        }
         run += tot;
     }
     if (blockIdx.x == G - 1 && threadIdx.x == 0) out[n] = bsum[G];
@@ -97,6 +116,23 @@ static void scan_run(const int *in, int *out, int n, int nonzero, int *scratch, 
 void gg_launch_scan(const int *in, int *out, int n, int *scratch, cudaStream_t st)
 {
     scan_run(in, out, n, 0, scratch, st);
+}
+
+#define GG_ORDER_MAX_LEVEL 14
+
+// cell level of the target order of system s: the deepest level whose cells
+// are still as large as the system's largest kernel radius, at most lmax
+__device__ __forceinline__ int target_order_level(const GGDomainDev *__restrict__ dom,
+                                                  const unsigned *__restrict__ hmm, int s, int lmax)
+{
+    const float hmax = __uint_as_float(hmm[2 * s + 1]);
+    const double len = dom[s].len;
+    int L = 0;
+    if (hmax > 0.f && isfinite(hmax))
+        while (L < lmax && ldexp(len, -(L + 1)) >= (double)hmax) L++;
+    else
+        L = lmax;
+    return L;
 }
 
 // ---- groups: ceil(n_s / gs) groups per system -------------------------------
@@ -146,6 +182,162 @@ void gg_launch_groups(const int *toff, int S, int gs, GGGroup *groups, int *ngro
     k_groups_count<<<1, 1024, 0, st>>>(toff, S, gs, gscan, ngroups);
     k_groups_write<<<gg_num_sms() * 8, 256, 0, st>>>(toff, gscan, S, gs, ngroups, groups);
     gg_note_launches(2);
+}
+
+// ---- groups bounded by tree nodes ------------------------------------------------
+// A group opens every node that reaches into the bounding box of its targets,
+// down to the particles for nodes inside the box.  Consecutive targets in key
+// order can still be far apart (the curve crosses sparse regions in long
+// strides), and then the box of a run of gs of them encloses dense regions none
+// of them belong to, which every target of the group opens to the particles: on
+// the 16.8M clustered system single groups of 64 outskirt targets, whose boxes
+// held 160,000-260,000 particles, ran longer than the rest of the walk together.
+// So a group never spans two "group nodes": the shallowest tree nodes holding at
+// most gs * GG_GROUP_NODE_GROUPS of the walk's targets, or lying at or below the
+// cell level the target order sorts by (targets ordered by softening class are
+// contiguous only per cell).  Within a group node the targets are cut into runs
+// of gs as before.  The rule depends on the system's own tree and targets only,
+// so a system's groups do not depend on the systems batched with it.
+#define GG_GROUP_NODE_GROUPS 64
+
+__device__ __forceinline__ bool group_node_pred(const TreeBuf &tb, const int *__restrict__ tscan, int k, int cap,
+                                                int lo)
+{
+    const int b = tb.start[k], e = tb.end[k];
+    const int targets = tscan ? tscan[e] - tscan[b] : e - b;
+    return targets <= cap || tb.level[k] >= lo;
+}
+
+// gnode[i] = the group node of sorted particle i.  tscan: exclusive count of
+// the walk's targets before each sorted particle (NULL: every particle is a
+// target).  A warp takes 32 nodes at a time and writes each group node's
+// particle range with all its lanes.
+__global__ void k_group_nodes(TreeBuf tb, const int *__restrict__ tscan, int gs, const GGDomainDev *__restrict__ dom,
+                              const unsigned *__restrict__ hmm, int lmax, int *__restrict__ gnode)
+{
+    const int nn = *tb.nnodes;
+    const int lane = threadIdx.x & 31;
+    const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    const int cap = GG_GROUP_NODE_GROUPS * gs;
+    for (int base = wg * 32; base < nn; base += nw * 32) {
+        const int k = base + lane;
+        bool is_gn = false;
+        if (k < nn) {
+            const int lo = dom ? target_order_level(dom, hmm, tb.sys[k], lmax) : INT_MAX;
+            const int par = tb.parent[k];
+            is_gn = group_node_pred(tb, tscan, k, cap, lo) && (par < 0 || !group_node_pred(tb, tscan, par, cap, lo));
+        }
+        unsigned m = __ballot_sync(0xffffffffu, is_gn);
+        while (m) {
+            const int j = __ffs(m) - 1;
+            m &= m - 1;
+            const int kk = base + j;
+            const int b = tb.start[kk], e = tb.end[kk];
+            for (int i = b + lane; i < e; i += 32) gnode[i] = kk;
+        }
+    }
+}
+
+// flag[t] = 1 where target t starts a new group node
+__global__ void k_group_seg_flags(int nt, const int *__restrict__ tlist, const int *__restrict__ gnode,
+                                  int *__restrict__ flag)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+        const int pi = tlist ? tlist[t] : t;
+        flag[t] = (t == 0 || gnode[pi] != gnode[tlist ? tlist[t - 1] : t - 1]) ? 1 : 0;
+    }
+}
+
+// segstart[j] = first target of segment j; segstart[nseg] = nt
+__global__ void k_group_seg_starts(int nt, const int *__restrict__ flag, const int *__restrict__ segidx,
+                                   int *__restrict__ segstart)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+        if (flag[t]) segstart[segidx[t]] = t;
+        if (t == 0) segstart[segidx[nt]] = nt;
+    }
+}
+
+// seg[t] becomes the segment holding target t, flag[t] 1 where t starts a
+// group: every gs-th target of its segment (both in place, one thread per t)
+__global__ void k_group_start_flags(int nt, int *__restrict__ flag, int *__restrict__ seg,
+                                    const int *__restrict__ segstart, int gs)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+        const int j = seg[t] + flag[t] - 1;
+        seg[t] = j;
+        flag[t] = ((t - segstart[j]) % gs) == 0 ? 1 : 0;
+    }
+}
+
+__global__ void k_group_write_tree(int nt, const int *__restrict__ flag, const int *__restrict__ seg,
+                                   const int *__restrict__ segstart, const int *__restrict__ gidx,
+                                   const int *__restrict__ toff, int S, int gs, int maxg, GGGroup *__restrict__ groups,
+                                   int *__restrict__ ngroups, int *__restrict__ err)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+        if (t == 0) *ngroups = min(gidx[nt], maxg);
+        if (!flag[t]) continue;
+        const int g = gidx[t];
+        if (g >= maxg) {   // cannot happen: the table is sized for the bound on group nodes
+            atomicOr(err, GG_EBIT_NODE_OVERFLOW);
+            continue;
+        }
+        const int j = seg[t];
+        int lo = 0, hi = S - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (toff[mid] <= t) lo = mid; else hi = mid - 1;
+        }
+        GGGroup gr;
+        gr.first = t;
+        gr.count = min(gs, segstart[j + 1] - t);
+        gr.root = lo;
+        gr.sys = lo;
+        groups[g] = gr;
+    }
+}
+
+// Upper bound of the number of groups: every group node is a root or a child
+// of a node holding more than gs * GG_GROUP_NODE_GROUPS targets (fewer than
+// n / (gs * GG_GROUP_NODE_GROUPS) per depth, at most 8 children each); each
+// adds at most one partial group to the n / gs full ones.
+long long gg_max_groups(long long n, int S, int gs)
+{
+    if (gs <= 1) return n + S + 1;
+    const long long per_depth = n / ((long long)gs * GG_GROUP_NODE_GROUPS) + 1;
+    return n / gs + 2LL * S + 1 + 8LL * GG_MAX_DEPTH * per_depth;
+}
+
+// Scratch: gnode n_particles + 1 ints (reused for the group index scan),
+// flag nt, seg and segstart nt + 1 each.
+void gg_launch_groups_tree(int nt, const int *tlist, const int *tscan, const int *toff, int S, int gs,
+                           const TreeBuf &tb, const GGDomainDev *order_dom, const unsigned *hmm, int lmax, int *gnode,
+                           int *flag, int *seg, int *segstart, int maxg, GGGroup *groups, int *ngroups,
+                           int *scan_scratch, int *err, cudaStream_t st)
+{
+    const int threads = 256, blocks = gg_num_sms() * 8;
+    if (nt <= 0) {
+        cudaMemsetAsync(ngroups, 0, sizeof(int), st);
+        return;
+    }
+    k_group_nodes<<<blocks, threads, 0, st>>>(tb, tscan, gs, order_dom, hmm, lmax, gnode);
+    k_group_seg_flags<<<blocks, threads, 0, st>>>(nt, tlist, gnode, flag);
+    scan_run(flag, seg, nt, 0, scan_scratch, st);
+    k_group_seg_starts<<<blocks, threads, 0, st>>>(nt, flag, seg, segstart);
+    k_group_start_flags<<<blocks, threads, 0, st>>>(nt, flag, seg, segstart, gs);
+    int *gidx = gnode;   // the group nodes are no longer needed
+    scan_run(flag, gidx, nt, 0, scan_scratch, st);
+    k_group_write_tree<<<blocks, threads, 0, st>>>(nt, flag, seg, segstart, gidx, toff, S, gs, maxg, groups, ngroups,
+                                                   err);
+    gg_note_launches(5);
+}
+
+int gg_target_order_lmax(int S)
+{
+    int sbits = 0;
+    while ((1 << sbits) < S) sbits++;
+    return std::min(GG_ORDER_MAX_LEVEL, (64 - 8 - sbits) / 3);
 }
 
 // ---- group order by measured cost -----------------------------------------------
@@ -450,7 +642,6 @@ extern "C" gg_status gg_fp32_peak_probe(double *tflops, void *stream)
 // radius, at most GG_ORDER_MAX_LEVEL), then softening class (quarter octaves of
 // h above the system's smallest), then key order.  Groups stay compact and are
 // homogeneous wherever a cell holds enough targets of one class.
-#define GG_ORDER_MAX_LEVEL 14
 __global__ void k_target_keys(int nt, const int *__restrict__ tlist, const GGPart *__restrict__ parts,
                               const unsigned long long *__restrict__ pkeys, const int *__restrict__ poff, int S,
                               const GGDomainDev *__restrict__ dom, const unsigned *__restrict__ hmm, int lmax,
@@ -464,13 +655,7 @@ __global__ void k_target_keys(int nt, const int *__restrict__ tlist, const GGPar
             if (__ldg(poff + mid) <= pi) lo = mid; else hi = mid - 1;
         }
         const unsigned hmin_bits = hmm[2 * lo];
-        const float hmax = __uint_as_float(hmm[2 * lo + 1]);
-        const double len = dom[lo].len;
-        int L = 0;
-        if (hmax > 0.f && isfinite(hmax))
-            while (L < lmax && ldexp(len, -(L + 1)) >= (double)hmax) L++;
-        else
-            L = lmax;
+        const int L = target_order_level(dom, hmm, lo, lmax);
         const unsigned long long cell = (pkeys[pi] >> (3 * (GG_MAX_LEVEL - L))) << (3 * (lmax - L));
         const unsigned hb = __float_as_uint(fmaxf(parts[pi].h, 0.f));
         const unsigned cls = hb > hmin_bits ? min((hb - hmin_bits) >> 21, 255u) : 0u;
@@ -498,7 +683,7 @@ gg_status gg_order_targets_by_softening(int nt, const int *tlist_in, const int *
     if (nt <= 0) return GG_OK;
     int sbits = 0;
     while ((1 << sbits) < S) sbits++;
-    const int lmax = std::min(GG_ORDER_MAX_LEVEL, (64 - 8 - sbits) / 3);
+    const int lmax = gg_target_order_lmax(S);
     const int key_bits = sbits + 3 * lmax + 8;
     int blocks = gg_num_sms() * 4;
     k_target_keys<<<blocks, 256, 0, st>>>(nt, tlist_in, parts, pkeys, poff, S, dom, hmm, lmax, key, val);

@@ -124,7 +124,10 @@ gg_status gg_synchronize(gg_ctx *ctx);
 gg_status gg_load_particles(gg_ctx *ctx, int32_t n_systems, const int64_t *counts, const double *pos,
                             int64_t pos_stride_bytes, const double *mass, int64_t mass_stride_bytes,
                             const double *soft_h, int64_t soft_stride_bytes);
-/* device-resident records {double x,y,z; float mass; float h} (32 bytes each) */
+/* device-resident records {double x,y,z; float mass; float h} (32 bytes each).
+ * Asynchronous on the context's stream: the per-system range of kernel radii
+ * (which decides whether walks order targets by softening) is copied to the
+ * host behind the load, and the first walk after it waits for that copy only. */
 gg_status gg_load_particles_device(gg_ctx *ctx, int32_t n_systems, const int64_t *counts, const void *d_records);
 
 /* ---- build -------------------------------------------------------------
