@@ -46,7 +46,7 @@ FLOPS_PER_INTERACTION = 20   # monopole force convention (3 sub, r^2, rsqrt, m/r
 # a 1-pass capture: 4.77 GB read + 1.67 GB written); on the galaxy from the
 # capture of the 1,000,000-particle galaxy (114.8 MB read + 39.6 MB written),
 # scaled to the 4.2M galaxy by particle count
-WALK_DRAM_BYTES_PER_PARTICLE = {"galaxy": 154.4, "galaxy1m": 154.4, "clustered": 6.44e9 / 16777216}
+WALK_DRAM_BYTES_PER_PARTICLE = {"galaxy": 154.4, "galaxy1m": 154.4, "clustered": 6.36e9 / 16777216}
 WALK_DRAM_SOURCE = {"galaxy": "ncu dram bytes of one k_walk launch on the 1M galaxy, scaled by N",
                     "galaxy1m": "ncu dram bytes of one k_walk launch on the 1M galaxy",
                     "clustered": "ncu dram bytes of one k_walk launch at full size (groups of 64; 1-pass capture)"}
