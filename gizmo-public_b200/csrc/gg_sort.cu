@@ -143,6 +143,7 @@ struct SortSmem {
     unsigned vals[SORT_TILE];
     unsigned short dig[SORT_TILE];
     unsigned whist[SORT_WARPS][RADIX];
+    unsigned bhist[RADIX];   // the tile's digit counts, published before the ranking
     unsigned texcl[RADIX];
     unsigned gbase[RADIX];
     unsigned wsum[SORT_WARPS];
@@ -163,6 +164,7 @@ __global__ void __launch_bounds__(SORT_THREADS, GG_SORT_MINB) k_sort_pass(
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     if (tid == 0) sm.tile = (int)atomicAdd(tile_counter, 1u);
     for (int i = tid; i < SORT_WARPS * RADIX; i += SORT_THREADS) (&sm.whist[0][0])[i] = 0;
+    for (int i = tid; i < RADIX; i += SORT_THREADS) sm.bhist[i] = 0;
     __syncthreads();
     const int tile = sm.tile;
     const long long tile_base = (long long)tile * SORT_TILE;
@@ -186,6 +188,17 @@ __global__ void __launch_bounds__(SORT_THREADS, GG_SORT_MINB) k_sort_pass(
         else if (sys_mode) d = ((unsigned)sort_sys_of(poff, S, v[j]) >> shift) & (RADIX - 1);
         else d = (unsigned)(k[j] >> shift) & (RADIX - 1);
         dg[j] = d;
+        atomicAdd(&sm.bhist[d], 1u);
+    }
+    // Early counts: the tile's per-digit counts (items past n counted under the
+    // last digit, as the ranking counts them) are published before the
+    // ranking, so that successors looking back find them sooner.
+    __syncthreads();
+    unsigned *st = status + (size_t)tile * RADIX;
+#pragma unroll
+    for (int q = 0; q < DPT; q++) {
+        const int d = DPT * tid + q;
+        st_status(&st[d], (tile == 0 ? ST_INC : ST_AGG) | (sm.bhist[d] & ST_VALUE));
     }
     // stable warp-level ranking in (item, lane) order == index order
 #pragma unroll
@@ -215,16 +228,12 @@ __global__ void __launch_bounds__(SORT_THREADS, GG_SORT_MINB) k_sort_pass(
         }
         sum[q] = acc;
     }
-    // publish and look back, digit by digit
-    unsigned *st = status + (size_t)tile * RADIX;
+    // look back, digit by digit, and publish the inclusive counts
 #pragma unroll
     for (int q = 0; q < DPT; q++) {
         const int d = DPT * tid + q;
         unsigned excl = 0;
-        if (tile == 0) {
-            st_status(&st[d], ST_INC | (sum[q] & ST_VALUE));
-        } else {
-            st_status(&st[d], ST_AGG | (sum[q] & ST_VALUE));
+        if (tile != 0) {
             int t = tile - 1;
             int spins = 0;
             while (t >= 0) {
