@@ -21,8 +21,8 @@
 #include "gg_kernels.cuh"
 
 // scratch of gg_sort_pairs_run for GG_NOALLOC_SORT_MAX_N pairs (12.6 MB for
-// the alternate keys and values, 1 MB of look-back status words with 4096-key
-// tiles and 9-bit digits), plus the error word in the last 256 bytes
+// the alternate keys and values, about 1 MB of look-back status words), plus
+// the error word in the last 256 bytes; the entry point checks the fit
 #define GG_NOALLOC_SCRATCH_BYTES (20u << 20)
 
 static __device__ __align__(256) unsigned char gg_noalloc_scratch[GG_NOALLOC_SCRATCH_BYTES];

@@ -7,7 +7,7 @@
 // SORT_TILE keys in shared memory, publishes its per-digit counts, sums its
 // predecessors' counts with a decoupled look-back, and writes the tile out
 // digit-sorted so that global stores are contiguous runs.  SORT_BITS-bit
-// digits (9: the 63-bit Peano-Hilbert keys take 7 passes).  For several
+// digits (8: the 63-bit Peano-Hilbert keys take 8 passes).  For several
 // systems further passes sort stably by system id (taken from the value, an
 // index into the concatenated particle array), so the final order is
 // (system, key).
@@ -26,14 +26,16 @@
 #include "gg_kernels.cuh"
 
 #ifndef GG_SORT_BITS
-#define GG_SORT_BITS 9
+#define GG_SORT_BITS 8
 #endif
-// 9-bit digits (7 passes for the 63-bit keys), 2048-key tiles, 4 blocks per
-// SM: measured best of {8,9} bits x {2048,3072,4096}-key tiles x 2-4 blocks per
-// SM on the 16.8M clustered system's keys (2.46 ms against 2.53 ms for 8-bit
-// digits; every variant within 12%: a pass is latency-bound, not tile-bound)
+// 8-bit digits (8 passes for the 63-bit keys), 2560-key tiles, 4 blocks per
+// SM: measured best on the 16.8M clustered system's keys with the vote-based
+// ranking, early counts and windowed look-back (ms per sort):
+//   9 bits x 2048 x 4: 2.11   9 x 3072 x 3: 1.90   9 x 4096 x 2: 1.98
+//   8 bits x 2048 x 4: 1.78   8 x 2560 x 4: 1.69   8 x 3072 x 3: 1.73   8 x 4096 x 2: 1.89
+// With match.any ranking 9 x 2048 x 4 had been best, at 2.46.
 #ifndef GG_SORT_ITEMS
-#define GG_SORT_ITEMS 8
+#define GG_SORT_ITEMS 10
 #endif
 #ifndef GG_SORT_MINB
 #define GG_SORT_MINB 4    // blocks per SM the pass kernel's registers must allow
@@ -51,6 +53,9 @@
 #define ST_FLAGS (3u << 30)
 #define ST_VALUE 0x3FFFFFFFu
 #define GG_SORT_SPIN_LIMIT (1 << 22)
+#ifndef GG_SORT_LB_WINDOW
+#define GG_SORT_LB_WINDOW 4   // predecessors read per look-back round trip
+#endif
 
 static_assert(RADIX >= SORT_THREADS && RADIX % SORT_THREADS == 0, "each thread owns whole digits");
 static_assert(SORT_BITS * GG_SORT_MAX_PASSES >= 64 + 32, "enough passes for a 64-bit key and a system id");
@@ -204,7 +209,14 @@ __global__ void __launch_bounds__(SORT_THREADS, GG_SORT_MINB) k_sort_pass(
 #pragma unroll
     for (int j = 0; j < SORT_ITEMS; j++) {
         const unsigned d = dg[j];
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        // lanes holding the same digit: one vote per digit bit (independent
+        // votes, cheaper here than match.any)
+        unsigned peers = 0xffffffffu;
+#pragma unroll
+        for (int b = 0; b < SORT_BITS; b++) {
+            const unsigned m = __ballot_sync(0xffffffffu, (d >> b) & 1u);
+            peers &= ((d >> b) & 1u) ? m : ~m;
+        }
         const int leader = __ffs(peers) - 1;
         unsigned base = 0;
         if (lane == leader) base = atomicAdd(&sm.whist[w][d], (unsigned)__popc(peers));
@@ -234,21 +246,36 @@ __global__ void __launch_bounds__(SORT_THREADS, GG_SORT_MINB) k_sort_pass(
         const int d = DPT * tid + q;
         unsigned excl = 0;
         if (tile != 0) {
+            // windowed look-back: GG_SORT_LB_WINDOW predecessors' words per
+            // round trip, taken in order until the first inclusive one; a word
+            // not yet published is polled again (bounded)
             int t = tile - 1;
             int spins = 0;
             while (t >= 0) {
-                const unsigned sv = ld_status(status + (size_t)t * RADIX + d);
-                if ((sv & ST_FLAGS) == 0u) {
+                unsigned w[GG_SORT_LB_WINDOW];
+#pragma unroll
+                for (int i = 0; i < GG_SORT_LB_WINDOW; i++)
+                    w[i] = t - i >= 0 ? ld_status(status + (size_t)(t - i) * RADIX + d) : ST_INC;
+                int used = 0;
+                bool done = false, waiting = false;
+#pragma unroll
+                for (int i = 0; i < GG_SORT_LB_WINDOW; i++) {
+                    if (done || waiting) continue;
+                    const unsigned f = w[i] & ST_FLAGS;
+                    if (f == 0u) { waiting = true; continue; }
+                    excl += w[i] & ST_VALUE;
+                    used++;
+                    if (f == ST_INC) done = true;
+                }
+                if (done) break;
+                t -= used;
+                if (waiting) {
                     if (++spins > GG_SORT_SPIN_LIMIT) {
                         atomicOr(err, GG_EBIT_SORT_TIMEOUT);
                         break;
                     }
                     __nanosleep(32);
-                    continue;
                 }
-                excl += sv & ST_VALUE;
-                if ((sv & ST_FLAGS) == ST_INC) break;
-                t--;
             }
             st_status(&st[d], ST_INC | ((excl + sum[q]) & ST_VALUE));
         }
