@@ -611,6 +611,7 @@ static TreeBuf tree_buf(gg_ctx *c)
     tb.sys = c->t_sys.p; tb.nch = c->t_nch.p; tb.child = c->t_child.p; tb.counter = c->t_counter.p;
     tb.bnd = c->t_bnd.p; tb.mass64 = c->t_mass64.p; tb.depth_beg = c->t_depth.p; tb.nnodes = c->t_nnodes.p;
     tb.blocksum = c->t_bsum.p; tb.blockoff = c->t_boff.p; tb.err = c->err.p;
+    tb.cap = c->ncap;
     return tb;
 }
 

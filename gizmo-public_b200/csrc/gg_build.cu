@@ -143,50 +143,6 @@ __global__ void __launch_bounds__(TB_THREADS) k_tree_count(int depth, const unsi
     if (threadIdx.x == 0) tb.blocksum[blockIdx.x] = s_sum;
 }
 
-// exclusive scan of the block sums, sets depth_beg[depth+2]
-__global__ void k_tree_scan(int depth, TreeBuf tb, int G, int cap)
-{
-    __shared__ int ws[32];
-    __shared__ int carry;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int base = 0; base < G; base += blockDim.x) {
-        int i = base + threadIdx.x;
-        int v = i < G ? tb.blocksum[i] : 0, x = v;
-        for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane == 31) ws[w] = x;
-        __syncthreads();
-        if (w == 0) {
-            int t = lane < nw ? ws[lane] : 0, u = t;
-            for (int o = 1; o < 32; o <<= 1) {
-                int y = __shfl_up_sync(0xffffffffu, u, o);
-                if (lane >= o) u += y;
-            }
-            if (lane < nw) ws[lane] = u - t;
-        }
-        __syncthreads();
-        if (i < G) tb.blockoff[i] = carry + x - v + ws[w];
-        __syncthreads();
-        if (threadIdx.x == blockDim.x - 1) carry += x + ws[w];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        int le = tb.depth_beg[depth + 1];
-        long long nxt = (long long)le + carry;
-        if (nxt > cap) {
-            atomicOr(tb.err, GG_EBIT_NODE_OVERFLOW);
-            nxt = le;   // drop the level; the host reports the overflow
-            for (int i = 0; i < G; i++) tb.blockoff[i] = 0;
-        }
-        tb.depth_beg[depth + 2] = (int)nxt;
-        tb.nnodes[0] = (int)nxt;
-    }
-}
-
 // Write phase: children of each node get contiguous indices after this depth.
 __global__ void __launch_bounds__(TB_THREADS) k_tree_write(int depth, const unsigned long long *__restrict__ keys,
                                                            TreeBuf tb, int leaf)
@@ -194,15 +150,45 @@ __global__ void __launch_bounds__(TB_THREADS) k_tree_write(int depth, const unsi
     __shared__ int s_nch[TB_NODES];
     __shared__ int s_excl[TB_NODES];
     __shared__ int s_tot;
+    __shared__ int s_red[2][TB_THREADS / 32];
     const int lb = tb.depth_beg[depth], le = tb.depth_beg[depth + 1];
-    const int next_end = tb.depth_beg[depth + 2];
-    if (next_end == le) return;   // no children at all (or dropped on overflow)
-    const int nl = le - lb;
     const int G = gridDim.x;
+    // this block's first child index and the depth's child total, summed from
+    // the count phase's per-block sums (G of them, in block order; exact)
+    {
+        int before = 0, all = 0;
+        for (int i = threadIdx.x; i < G; i += TB_THREADS) {
+            const int v = tb.blocksum[i];
+            all += v;
+            if (i < (int)blockIdx.x) before += v;
+        }
+        before = __reduce_add_sync(0xffffffffu, before);
+        all = __reduce_add_sync(0xffffffffu, all);
+        if ((threadIdx.x & 31) == 0) { s_red[0][threadIdx.x >> 5] = before; s_red[1][threadIdx.x >> 5] = all; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int bsum = 0, tsum = 0;
+            for (int w = 0; w < TB_THREADS / 32; w++) { bsum += s_red[0][w]; tsum += s_red[1][w]; }
+            long long nxt = (long long)le + tsum;
+            const bool over = nxt > tb.cap;
+            if (over) nxt = le;   // drop the level; the host reports the overflow
+            if (blockIdx.x == 0) {
+                if (over) atomicOr(tb.err, GG_EBIT_NODE_OVERFLOW);
+                tb.depth_beg[depth + 2] = (int)nxt;
+                tb.nnodes[0] = (int)nxt;
+            }
+            s_tot = over ? 0 : tsum;
+            s_red[0][0] = bsum;
+        }
+        __syncthreads();
+    }
+    if (s_tot == 0) return;   // no children at all (or dropped on overflow)
+    const int nl = le - lb;
     const int chunk = (nl + G - 1) / G;
     const int cb = lb + blockIdx.x * chunk, ce = min(le, cb + chunk);
     const int g = threadIdx.x / TB_GROUP, j = threadIdx.x % TB_GROUP;
-    int run = le + tb.blockoff[blockIdx.x];
+    int run = le + s_red[0][0];
+    __syncthreads();   // s_tot is reused below
     for (int base = cb; base < ce; base += TB_NODES) {
         int k = base + g;
         bool valid = k < ce;
@@ -342,13 +328,13 @@ void gg_launch_tree(const unsigned long long *keys, const int *poff, int S, int 
 {
     const int G = gg_tree_grid();
     k_tree_roots<<<(S + 127) / 128, 128, 0, st>>>(S, poff, tb);
+    tb.cap = cap;
     for (int depth = 0; depth < GG_MAX_DEPTH; depth++) {
         k_tree_count<<<G, TB_THREADS, 0, st>>>(depth, keys, tb, leaf);
-        k_tree_scan<<<1, 1024, 0, st>>>(depth, tb, G, cap);
         k_tree_write<<<G, TB_THREADS, 0, st>>>(depth, keys, tb, leaf);
     }
     const int threads = 256, blocks = gg_num_sms() * 8;
     for (int depth = GG_MAX_DEPTH - 1; depth >= 0; depth--)
         k_tree_moments_depth<<<blocks, threads, 0, st>>>(depth, parts, dom, tb, nodes);
-    gg_note_launches(1 + 4 * GG_MAX_DEPTH);
+    gg_note_launches(1 + 3 * GG_MAX_DEPTH);
 }

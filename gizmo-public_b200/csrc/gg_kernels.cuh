@@ -12,6 +12,7 @@ struct TreeBuf {
     int *depth_beg;    // GG_MAX_DEPTH + 2 entries
     int *nnodes;       // total nodes (device)
     int *blocksum, *blockoff;
+    int cap;           // node capacity (set by gg_launch_tree)
     int *err;
 };
 
