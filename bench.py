@@ -591,9 +591,12 @@ def run_serve(args, torch, ggb200, dist, world, rank, local):
     pool = ics.serving_pool(n_systems=128, seed=multi.rank_seed(ics.SEED_SERVING, rank))
     trace = serve.make_trace(pool, rate=2000.0, window_s=args.serve_window, frac_reeval=0.3, dt=1e-3, recent=64,
                              seed=multi.rank_seed(ics.SEED_SERVING, rank) + 1)
-    # warm-up: library, contexts and pinned staging on a short offline slice
+    # warm-up on an offline slice of the trace: the library, the contexts, and
+    # the process's cache of pinned staging blocks, which then holds blocks of
+    # every size the batches ask for, as a long-running server's would
+    # (page-locking them costs host time the first time only)
     warm = serve.Server(budget_bytes=120e9, tol=args.tol, reserve=True)   # maps the 120 GB budget once
-    serve.run_trace(warm, _copy_trace(trace[:max(3, args.warmup) * 100]), realtime=False)
+    serve.run_trace(warm, _copy_trace(trace[:max(3, args.warmup) * 250]), realtime=False)
     warm.close()
     torch.cuda.synchronize()
 

@@ -74,7 +74,7 @@ class _Context:
 
 class Server:
     def __init__(self, budget_bytes=120e9, tol=0.001, batching=True, max_batch_particles=8 << 20,
-                 max_batch_systems=1024, max_inflight=6, leaf=8, group=32, flush=128, device=0, tree_factory=None,
+                 max_batch_systems=1024, max_inflight=16, leaf=8, group=32, flush=128, device=0, tree_factory=None,
                  threaded=False, reserve=False):
         self.budget = float(budget_bytes)
         self.tol = tol
