@@ -274,6 +274,7 @@ struct gg_ctx {
     HostBuf<double> h_acc, h_pot, h_old;
     long long async_n = 0;
     int async_flags = 0;
+    bool async_pinned = false;             // the last async walk copied into the caller's pinned arrays
     cudaEvent_t act_ev = nullptr, done_ev = nullptr;
     // host OldAcc of gg_evaluate crosses the link on its own stream into its
     // own array, while the build runs; the walk waits for it (old_ready_ev) and
@@ -1615,8 +1616,11 @@ extern "C" gg_status gg_load_system_velocities(gg_ctx *c, const double *const *v
 }
 
 // ---------------------------------------------------------------- asynchronous evaluation
-extern "C" gg_status gg_evaluate_async(gg_ctx *c, const int32_t *active, int64_t n_active, double tol, double theta,
-                                       int32_t flags)
+// the asynchronous walk; with acc_pinned / pot_pinned (pinned mode) the
+// results go straight to the caller's page-locked arrays, otherwise per flags
+// into the context's own pinned buffers
+static gg_status evaluate_async(gg_ctx *c, const int32_t *active, int64_t n_active, double tol, double theta,
+                                int32_t flags, bool pinned, double *acc_pinned, double *pot_pinned)
 {
     if (!c) return GG_ERR_INVALID;
     if (!c->built) return GG_ERR_NOT_BUILT;
@@ -1624,6 +1628,17 @@ extern "C" gg_status gg_evaluate_async(gg_ctx *c, const int32_t *active, int64_t
     if (flags & ~(GG_ASYNC_COPY_ACC | GG_ASYNC_COPY_POT)) return GG_ERR_INVALID;
     gg_status st;
     if ((st = set_device(c))) return st;
+    if (pinned) {
+        for (const void *ptr : {(const void *)acc_pinned, (const void *)pot_pinned}) {
+            if (!ptr) continue;
+            cudaPointerAttributes a;
+            if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+                cudaGetLastError();
+                return GG_ERR_INVALID;
+            }
+            if (a.type != cudaMemoryTypeHost) return GG_ERR_INVALID;
+        }
+    }
     cudaStream_t s = c->stream;
     const long long nt = active ? n_active : c->N;
     size_t outn = (size_t)(c->N > 0 ? c->N : 1);
@@ -1639,7 +1654,15 @@ extern "C" gg_status gg_evaluate_async(gg_ctx *c, const int32_t *active, int64_t
         d_active = c->active_d.p;
     }
     if ((st = run_walk(c, d_active, (int)n_active, nullptr, tol, theta, c->acc_d.p, c->pot_d.p, nullptr))) return st;
-    if (flags) {
+    c->async_pinned = pinned;
+    if (pinned) {
+        if (nt && acc_pinned)
+            GG_CUDA_TRY(cudaMemcpyAsync(acc_pinned, c->acc_d.p, nt * 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (nt && pot_pinned)
+            GG_CUDA_TRY(cudaMemcpyAsync(pot_pinned, c->pot_d.p, nt * sizeof(double), cudaMemcpyDeviceToHost, s));
+        c->async_n = nt;
+        c->async_flags = 0;
+    } else if (flags) {
         // unfetched results of an earlier call are overwritten in stream order
         if ((flags & GG_ASYNC_COPY_ACC) && (st = c->h_acc.ensure((size_t)nt * 3, c->done_ev))) return st;
         if ((flags & GG_ASYNC_COPY_POT) && (st = c->h_pot.ensure((size_t)nt, c->done_ev))) return st;
@@ -1652,6 +1675,51 @@ extern "C" gg_status gg_evaluate_async(gg_ctx *c, const int32_t *active, int64_t
     }
     c->last.n_targets = nt;
     GG_CUDA_TRY(cudaEventRecord(c->done_ev, s));
+    return GG_OK;
+}
+
+extern "C" gg_status gg_evaluate_async(gg_ctx *c, const int32_t *active, int64_t n_active, double tol, double theta,
+                                       int32_t flags)
+{
+    return evaluate_async(c, active, n_active, tol, theta, flags, false, nullptr, nullptr);
+}
+
+extern "C" gg_status gg_evaluate_async_pinned(gg_ctx *c, const int32_t *active, int64_t n_active, double tol,
+                                              double theta, double *acc_pinned, double *pot_pinned)
+{
+    return evaluate_async(c, active, n_active, tol, theta, 0, true, acc_pinned, pot_pinned);
+}
+
+// page-locked blocks handed to callers: pointer -> block size
+static std::mutex g_user_pinned_mu;
+static std::map<void *, size_t> g_user_pinned;
+
+extern "C" gg_status gg_host_alloc(int64_t bytes, void **out)
+{
+    if (!out || bytes < 0) return GG_ERR_INVALID;
+    size_t got = 0;
+    void *p = pinned_get(bytes > 0 ? (size_t)bytes : 1, &got);
+    if (!p) return GG_ERR_NOMEM;
+    {
+        std::lock_guard<std::mutex> lk(g_user_pinned_mu);
+        g_user_pinned[p] = got;
+    }
+    *out = p;
+    return GG_OK;
+}
+
+extern "C" gg_status gg_host_free(void *ptr)
+{
+    if (!ptr) return GG_OK;
+    size_t bytes = 0;
+    {
+        std::lock_guard<std::mutex> lk(g_user_pinned_mu);
+        auto it = g_user_pinned.find(ptr);
+        if (it == g_user_pinned.end()) return GG_ERR_INVALID;
+        bytes = it->second;
+        g_user_pinned.erase(it);
+    }
+    pinned_put(ptr, bytes);
     return GG_OK;
 }
 
@@ -1671,6 +1739,7 @@ extern "C" gg_status gg_fetch_results(gg_ctx *c, double *acc_out, double *pot_ou
     if ((st = set_device(c))) return st;
     GG_CUDA_TRY(cudaEventSynchronize(c->done_ev));
     const long long nt = c->async_n;
+    if (c->async_pinned && (acc_out || pot_out)) return GG_ERR_INVALID;   // already in the caller's arrays
     if (acc_out) {
         if (!(c->async_flags & GG_ASYNC_COPY_ACC)) return GG_ERR_INVALID;
         parallel_copy(acc_out, c->h_acc.p, (size_t)nt * 3 * sizeof(double));

@@ -14,6 +14,7 @@ import os
 import re
 import subprocess
 import threading
+import weakref
 
 import numpy as np
 
@@ -132,6 +133,9 @@ def load_library():
             "gg_evaluate_async": (i32, [P, P, i64, dbl, dbl, i32]),
             "gg_query": (i32, [P]),
             "gg_fetch_results": (i32, [P, P, P, ctypes.POINTER(Stats)]),
+            "gg_evaluate_async_pinned": (i32, [P, P, i64, dbl, dbl, P, P]),
+            "gg_host_alloc": (i32, [i64, ctypes.POINTER(P)]),
+            "gg_host_free": (i32, [P]),
             "gg_drift_systems": (i32, [P, P]),
             "gg_graph_capture_step": (i32, [P, dbl, dbl, P, P]),
             "gg_graph_launch": (i32, [P]),
@@ -194,6 +198,7 @@ class GravityTree:
         self._lib, self._h = lib, h
         self.n = 0
         self.counts = None
+        self._pinned_out = None
 
     def close(self):
         if self._h:
@@ -321,6 +326,7 @@ class GravityTree:
                                            err_tol_theta, flags), "gg_evaluate_async")
         self._async_n = self.n if act is None else n
         self._async_flags = flags
+        self._pinned_out = None
 
     def query(self):
         """True when the last asynchronous evaluation has finished."""
@@ -330,8 +336,30 @@ class GravityTree:
         _check(st, "gg_query")
         return True
 
+    def evaluate_async_pinned(self, acc, pot, active=None, err_tol_force_acc=0.0025, err_tol_theta=0.0):
+        """Queue a walk whose results are copied straight into `acc` (n, 3) and
+        `pot` (n), page-locked arrays from host_empty (either may be None);
+        fetch() then only waits and returns them."""
+        act = None if active is None else np.ascontiguousarray(active, dtype=np.int32)
+        n = self.n if act is None else act.shape[0]
+        for a, shape in ((acc, (n, 3)), (pot, (n,))):
+            if a is not None and (a.dtype != np.float64 or a.shape != shape or not a.flags.c_contiguous):
+                raise ValueError("pinned result array must be C-contiguous float64 of shape %s" % (shape,))
+        _check(self._lib.gg_evaluate_async_pinned(self._h, None if act is None else act.ctypes.data, 0 if act is None
+                                                  else n, err_tol_force_acc, err_tol_theta, _ptr(acc), _ptr(pot)),
+               "gg_evaluate_async_pinned")
+        self._async_n = n
+        self._async_flags = 0
+        self._pinned_out = (acc, pot)
+
     def fetch(self):
         """Wait for the last asynchronous evaluation; returns (acc, pot, stats)."""
+        if self._pinned_out is not None:
+            acc, pot = self._pinned_out
+            self._pinned_out = None
+            st = Stats()
+            _check(self._lib.gg_fetch_results(self._h, None, None, ctypes.byref(st)), "gg_fetch_results")
+            return acc, pot, st.as_dict()
         n = self._async_n
         acc = np.empty((n, 3)) if self._async_flags & ASYNC_COPY_ACC else None
         pot = np.empty(n) if self._async_flags & ASYNC_COPY_POT else None
@@ -492,6 +520,20 @@ def direct_sum_fp64(d_pos, d_mass, d_h, n_src, d_targets, n_tgt, d_acc, d_pot, s
     lib = load_library()
     _check(lib.gg_direct_sum_fp64(n_src, _ptr(d_pos), _ptr(d_mass), _ptr(d_h), n_tgt, _ptr(d_targets), _ptr(d_acc),
                                   _ptr(d_pot), stream), "gg_direct_sum_fp64")
+
+
+def host_empty(shape, dtype=np.float64):
+    """A numpy array in a page-locked block of the library's host cache
+    (gg_host_alloc); the block goes back to the cache when the array and every
+    view of it are gone."""
+    lib = load_library()
+    dt = np.dtype(dtype)
+    nbytes = int(np.prod(shape)) * dt.itemsize
+    p = ctypes.c_void_p()
+    _check(lib.gg_host_alloc(max(nbytes, 1), ctypes.byref(p)), "gg_host_alloc")
+    buf = (ctypes.c_char * max(nbytes, 1)).from_address(p.value)
+    weakref.finalize(buf, lib.gg_host_free, ctypes.c_void_p(p.value))
+    return np.frombuffer(buf, dtype=dt, count=int(np.prod(shape))).reshape(shape)
 
 
 def reserve_device_pool(nbytes, device=0):

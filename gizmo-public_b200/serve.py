@@ -25,8 +25,15 @@ launch sequence, with the same library calls.
 
 Finished launches are fetched (results copied out of the library's pinned
 buffers by all host threads) by the scheduler itself; threaded=True hands the
-fetches to a completion thread instead, which helps only where the host has
-cores to spare for two concurrent OpenMP copies.
+fetches to a completion thread instead.  With pinned_results=True the relative
+pass copies its results straight into page-locked arrays allocated for that
+launch (ggb200.host_empty, from the library's host cache) and each request's
+results are views of them, so a finished launch costs the scheduler no host
+copy.  That pays only where requests' results are released as they are
+consumed, so that the blocks go back to the cache: a caller that keeps every
+result makes each launch page-lock fresh memory, which costs far more than
+the copy (the 2,000 req/s benchmark trace, which keeps all results, ran 4x
+slower so).
 
 The latency of a request is from its arrival to its result in host memory.
 """
@@ -75,7 +82,7 @@ class _Context:
 class Server:
     def __init__(self, budget_bytes=120e9, tol=0.001, batching=True, max_batch_particles=8 << 20,
                  max_batch_systems=1024, max_inflight=16, leaf=8, group=32, flush=128, device=0, tree_factory=None,
-                 threaded=False, reserve=False):
+                 threaded=False, reserve=False, pinned_results=False, result_alloc=None):
         self.budget = float(budget_bytes)
         self.tol = tol
         self.batching = batching
@@ -84,6 +91,8 @@ class Server:
         self.max_inflight = int(max_inflight) if batching else 1
         self.cfg = dict(leaf_size=leaf, group_size=group, flush=flush, device=device)
         self.tree_factory = tree_factory or ggb200.GravityTree
+        self.pinned_results = pinned_results
+        self.result_alloc = result_alloc or ggb200.host_empty   # page-locked result arrays (pinned_results)
         if reserve:
             # map the whole budget once, before the first request; a device
             # smaller than the budget keeps what it could map, and admission
@@ -192,7 +201,11 @@ class Server:
         t.load_systems(systems)
         t.build()
         t.evaluate_async(err_tol_theta=STARTUP_THETA, copy_acc=False, copy_pot=False)
-        t.evaluate_async(err_tol_force_acc=self.tol, err_tol_theta=0.0)
+        if self.pinned_results:
+            t.evaluate_async_pinned(self.result_alloc((n, 3)), self.result_alloc(n), err_tol_force_acc=self.tol,
+                                    err_tol_theta=0.0)
+        else:
+            t.evaluate_async(err_tol_force_acc=self.tol, err_tol_theta=0.0)
         c.sids = [r.rid if r.kind == "new" else r.target for r in reqs]
         c.offsets = np.concatenate([[0], np.cumsum([r.n for r in reqs])])
         c.busy = True
@@ -215,7 +228,12 @@ class Server:
             items.append((r, k))
         t = c.tree
         t.drift(dts)
-        t.evaluate_async(active=np.concatenate(active), err_tol_force_acc=self.tol, err_tol_theta=0.0)
+        act = np.concatenate(active)
+        if self.pinned_results:
+            t.evaluate_async_pinned(self.result_alloc((act.size, 3)), self.result_alloc(act.size), active=act,
+                                    err_tol_force_acc=self.tol, err_tol_theta=0.0)
+        else:
+            t.evaluate_async(active=act, err_tol_force_acc=self.tol, err_tol_theta=0.0)
         c.busy = True
         c.last_use = now
         for r, k in group:

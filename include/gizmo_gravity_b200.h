@@ -248,6 +248,22 @@ gg_status gg_evaluate_async(gg_ctx *ctx, const int32_t *active, int64_t n_active
                             double err_tol_theta, int32_t flags);
 gg_status gg_query(gg_ctx *ctx);
 gg_status gg_fetch_results(gg_ctx *ctx, double *acc_out, double *pot_out, gg_stats *stats);
+/* The same walk with the results copied straight into the caller's
+ * page-locked host arrays (acc n*3, pot n; either may be NULL), so that
+ * gg_fetch_results only waits and returns the stats (its acc_out and pot_out
+ * must then be NULL).  The arrays must stay allocated until the fetch; a host
+ * array that is not page-locked is refused with GG_ERR_INVALID.  A serving
+ * loop that hands each request a view of its batch's result block saves the
+ * copy out of the context's own pinned buffers, which otherwise takes a host
+ * thread's time at memory bandwidth. */
+gg_status gg_evaluate_async_pinned(gg_ctx *ctx, const int32_t *active, int64_t n_active, double err_tol_force_acc,
+                                   double err_tol_theta, double *acc_pinned, double *pot_pinned);
+/* Page-locked host blocks from the library's process-wide cache (the one its
+ * contexts stage transfers through): gg_host_alloc returns a block of at least
+ * `bytes`, gg_host_free gives it back to the cache (GG_ERR_INVALID for a
+ * pointer gg_host_alloc did not return).  Thread-safe. */
+gg_status gg_host_alloc(int64_t bytes, void **out);
+gg_status gg_host_free(void *ptr);
 
 /* ---- batched steps ------------------------------------------------------
  * No counterpart in the reference, which walks one system per process.  A

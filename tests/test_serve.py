@@ -109,3 +109,42 @@ def test_device_pool_reservation():
     ggb200.reserve_device_pool(1 << 30)      # served from the pool the second time
     with pytest.raises(ggb200.GravityError):
         ggb200.reserve_device_pool(-1)
+
+
+def test_pinned_results_equal_the_copied_ones():
+    """gg_evaluate_async_pinned writes the same bits into the caller's
+    page-locked arrays as gg_evaluate_async + gg_fetch_results copy out (two
+    contexts taken through the same steps), for all targets and then an active
+    subset; a pageable array is refused; gg_host_free refuses a pointer that
+    is not one of its blocks."""
+    import ctypes
+    import ggb200
+    sysd = ics.serving_system(0, 20000, 601)
+    act = np.sort(np.random.default_rng(602).choice(20000, 3000, replace=False)).astype(np.int32)
+    res = []
+    for pinned in (False, True):
+        with ggb200.GravityTree() as t:
+            t.load_systems([sysd])
+            t.build()
+            t.evaluate_async(err_tol_theta=0.7, copy_acc=False, copy_pot=False)
+            t.fetch()
+            out = []
+            for active in (None, act):
+                n = 20000 if active is None else act.size
+                if pinned:
+                    acc, pot = ggb200.host_empty((n, 3)), ggb200.host_empty(n)
+                    t.evaluate_async_pinned(acc, pot, active=active, err_tol_force_acc=0.001)
+                    a, p, st = t.fetch()
+                    assert a is acc and p is pot
+                else:
+                    t.evaluate_async(active=active, err_tol_force_acc=0.001)
+                    a, p, st = t.fetch()
+                assert st["n_targets"] == n
+                out.append((a, p, st["interactions"]))
+            if pinned:
+                with pytest.raises(ggb200.GravityError):
+                    t.evaluate_async_pinned(np.empty((20000, 3)), None, err_tol_force_acc=0.001)
+            res.append(out)
+    for (a0, p0, i0), (a1, p1, i1) in zip(*res):
+        assert np.array_equal(a0, a1) and np.array_equal(p0, p1) and i0 == i1
+    assert ggb200.load_library().gg_host_free(ctypes.c_void_p(0x1000)) == -1

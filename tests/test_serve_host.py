@@ -55,12 +55,22 @@ class FakeTree:
         self.result = (self.pos[idx] - cent[sys_of], np.full(idx.size, float(self.counts.size > 0)) * sys_of * 0)
         self.left = int(self.polls_rng.integers(1, 5))
 
+    def evaluate_async_pinned(self, acc, pot, active=None, err_tol_force_acc=0.0, err_tol_theta=0.0):
+        self.evaluate_async(active, err_tol_force_acc, err_tol_theta)
+        self.out = (acc, pot)
+
     def query(self):
         self.left -= 1
         return self.left <= 0
 
     def fetch(self):
         acc, pot = self.result
+        if getattr(self, "out", None) is not None:
+            a, p = self.out
+            self.out = None
+            a[:] = acc
+            p[:] = pot + 1.0
+            return a, p, {"error_word": 0}
         return acc.copy(), pot.copy() + 1.0, {"error_word": 0}
 
     def device_bytes(self):
@@ -97,7 +107,8 @@ def _expected(reqs):
 def test_every_request_gets_its_own_result(batching):
     pool = _pool()
     reqs = serve.make_trace(pool, rate=1e6, window_s=3e-4, frac_reeval=0.4, dt=1e-2, recent=5, seed=3)[:80]
-    srv = serve.Server(batching=batching, max_batch_particles=6000, max_inflight=3, tree_factory=FakeTree)
+    srv = serve.Server(batching=batching, max_batch_particles=6000, max_inflight=3, tree_factory=FakeTree,
+                       pinned_results=batching, result_alloc=np.empty)
     serve.run_trace(srv, reqs, realtime=False)
     exp = _expected(reqs)
     for r in reqs:
@@ -118,7 +129,7 @@ def test_budget_is_respected_and_misses_are_resolved():
     pool = _pool(k=12, seed=12)
     budget = 3 * (FakeTree.fixed + FakeTree.bytes_per_particle * 6000)
     srv = serve.Server(budget_bytes=budget, batching=True, max_batch_particles=6000, max_inflight=2,
-                       tree_factory=FakeTree)
+                       tree_factory=FakeTree, result_alloc=np.empty)
     first = [serve.Request(i, "new", 0.0, system=pool[i]) for i in range(12)]
     serve.run_trace(srv, first, realtime=False)
     # the earliest systems were evicted to make room: their re-evaluations miss
@@ -137,7 +148,7 @@ def test_budget_is_respected_and_misses_are_resolved():
 def test_request_larger_than_the_budget_is_refused():
     pool = _pool(k=1, seed=13)
     reqs = [serve.Request(0, "new", 0.0, system=pool[0])]
-    srv = serve.Server(budget_bytes=1e6, tree_factory=FakeTree)
+    srv = serve.Server(budget_bytes=1e6, tree_factory=FakeTree, result_alloc=np.empty)
     with pytest.raises(MemoryError):
         serve.run_trace(srv, reqs, realtime=False)
 
