@@ -38,7 +38,8 @@ def _steps(ic, group_order, active=None, potential=False):
         t.build()
         t.evaluate_device(acc, pot, d_active=d_act, n_active=n_act, err_tol_force_acc=0.001, d_ninter=nint)
         stream.synchronize()
-        out.append((acc.cpu().numpy().copy(), pot.cpu().numpy().copy(), nint.cpu().numpy().copy()))
+        m = n if active is None else n_act   # a subset walk writes its first n_act slots only
+        out.append((acc[:m].cpu().numpy().copy(), pot[:m].cpu().numpy().copy(), nint[:m].cpu().numpy().copy()))
     if potential:
         t.evaluate_potential_device(pot)
         stream.synchronize()
