@@ -213,8 +213,8 @@ struct gg_ctx {
     DevBuf<char> sort_scratch;
     // tree
     int ncap = 0;
-    DevBuf<int> t_start, t_end, t_level, t_parent, t_sys, t_nch, t_child, t_counter, t_bnd, t_depth, t_nnodes,
-        t_bsum, t_boff;
+    DevBuf<int> t_start, t_end, t_level, t_parent, t_sys, t_nch, t_child, t_bnd, t_depth, t_nnodes;
+    DevBuf<unsigned> t_bstat, t_ticket;
     DevBuf<double> t_mass64;
     DevBuf<GGNode> nodes;
     // walk
@@ -290,8 +290,8 @@ struct gg_ctx {
     {
         f(poff); f(in_rec); f(part); f(dom); f(extent_mm); f(hmm); f(tkey); f(tval); f(tlist2); f(tout2);
         f(keys); f(perm); f(rank); f(sort_scratch);
-        f(t_start); f(t_end); f(t_level); f(t_parent); f(t_sys); f(t_nch); f(t_child); f(t_counter); f(t_bnd);
-        f(t_depth); f(t_nnodes); f(t_bsum); f(t_boff); f(t_mass64); f(nodes);
+        f(t_start); f(t_end); f(t_level); f(t_parent); f(t_sys); f(t_nch); f(t_child); f(t_bnd);
+        f(t_depth); f(t_nnodes); f(t_bstat); f(t_ticket); f(t_mass64); f(nodes);
         f(oldacc); f(vel); f(newpos); f(kin); f(kin_counter); f(dts); f(oldacc_save); f(tcost); f(gkey); f(gorder);
         f(e_chunks); f(e_first); f(e_part); f(e_out);
         f(groups); f(ngroups); f(gscan); f(toff); f(flag); f(flagscan); f(tlist); f(tout); f(scan_scratch);
@@ -597,9 +597,10 @@ static gg_status ensure_tree(gg_ctx *c)
     int G = gg_tree_grid();
     if ((st = c->t_start.ensure(cap)) || (st = c->t_end.ensure(cap)) || (st = c->t_level.ensure(cap)) ||
         (st = c->t_parent.ensure(cap)) || (st = c->t_sys.ensure(cap)) || (st = c->t_nch.ensure(cap)) ||
-        (st = c->t_child.ensure(cap)) || (st = c->t_counter.ensure(cap)) || (st = c->t_bnd.ensure(cap * 8)) ||
+        (st = c->t_child.ensure(cap)) || (st = c->t_bnd.ensure(cap * 8)) ||
         (st = c->t_mass64.ensure(cap)) || (st = c->nodes.ensure(cap)) || (st = c->t_depth.ensure(GG_MAX_DEPTH + 4)) ||
-        (st = c->t_nnodes.ensure(4)) || (st = c->t_bsum.ensure(G + 4)) || (st = c->t_boff.ensure(G + 4)))
+        (st = c->t_nnodes.ensure(4)) || (st = c->t_bstat.ensure((size_t)GG_MAX_DEPTH * G)) ||
+        (st = c->t_ticket.ensure(GG_MAX_DEPTH)))
         return st;
     c->ncap = (int)cap;
     return GG_OK;
@@ -609,9 +610,9 @@ static TreeBuf tree_buf(gg_ctx *c)
 {
     TreeBuf tb;
     tb.start = c->t_start.p; tb.end = c->t_end.p; tb.level = c->t_level.p; tb.parent = c->t_parent.p;
-    tb.sys = c->t_sys.p; tb.nch = c->t_nch.p; tb.child = c->t_child.p; tb.counter = c->t_counter.p;
+    tb.sys = c->t_sys.p; tb.nch = c->t_nch.p; tb.child = c->t_child.p;
     tb.bnd = c->t_bnd.p; tb.mass64 = c->t_mass64.p; tb.depth_beg = c->t_depth.p; tb.nnodes = c->t_nnodes.p;
-    tb.blocksum = c->t_bsum.p; tb.blockoff = c->t_boff.p; tb.err = c->err.p;
+    tb.bstat = c->t_bstat.p; tb.ticket = c->t_ticket.p; tb.err = c->err.p;
     tb.cap = c->ncap;
     return tb;
 }

@@ -56,7 +56,6 @@ __global__ void k_tree_roots(int S, const int *__restrict__ poff, TreeBuf tb)
     tb.level[s] = 0;
     tb.parent[s] = -1;
     tb.sys[s] = s;
-    tb.counter[s] = 0;
 }
 
 // deepest common level of two keys (0..21)
@@ -94,22 +93,59 @@ __device__ __forceinline__ int chunk_children(int cnt, int leaf)
     return (cnt + sz - 1) / sz;
 }
 
-// Count phase for one depth: 8 threads per node find the 7 digit boundaries;
-// per-block sums of child counts go to blocksum[blockIdx.x].
-__global__ void __launch_bounds__(TB_THREADS) k_tree_count(int depth, const unsigned long long *__restrict__ keys,
+__device__ __forceinline__ unsigned tb_ld_status(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void tb_st_status(unsigned *p, unsigned v)
+{
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+#define TB_PUBLISHED 0x80000000u
+#define TB_SPIN_LIMIT (1 << 22)
+
+// One depth of the build in one launch.  Blocks take their chunk of the
+// depth's nodes in ticket order (an atomic counter, so that every block a
+// block waits for has already started).  Count: 8 threads per node find the
+// 7 digit boundaries (or the chunk split of a full-depth cell) and the child
+// count; the block publishes its children total.  Then each block adds up the
+// totals of the blocks before it -- they publish before they wait on anyone,
+// so the bounded wait ends -- and writes its nodes' children at contiguous
+// indices from there; the last block also sets the next depth's range.  A
+// child index at or past the node capacity is not written and sets
+// GG_EBIT_NODE_OVERFLOW (the capacity is sized so that it cannot happen).
+__global__ void __launch_bounds__(TB_THREADS) k_tree_depth(int depth, const unsigned long long *__restrict__ keys,
                                                            TreeBuf tb, int leaf)
 {
-    __shared__ int s_sum;
+    __shared__ int s_sum, s_ticket, s_off, s_tot;
+    __shared__ int s_red[TB_THREADS / 32];
+    __shared__ int s_nch[TB_NODES];
+    __shared__ int s_excl[TB_NODES];
     const int lb = tb.depth_beg[depth], le = tb.depth_beg[depth + 1];
     const int nl = le - lb;
     const int G = gridDim.x;
-    const int chunk = (nl + G - 1) / G;
-    const int cb = lb + blockIdx.x * chunk, ce = min(le, cb + chunk);
-    if (threadIdx.x == 0) s_sum = 0;
+    if (threadIdx.x == 0) {
+        s_ticket = (int)atomicAdd(tb.ticket + depth, 1u);
+        s_sum = 0;
+    }
     __syncthreads();
+    const int blk = s_ticket;
+    if (nl == 0) {   // nothing at this depth: the next one is empty too
+        if (blk == G - 1 && threadIdx.x == 0) {
+            tb.depth_beg[depth + 2] = le;
+            tb.nnodes[0] = le;
+        }
+        return;
+    }
+    const int chunk = (nl + G - 1) / G;
+    const int cb = lb + blk * chunk, ce = min(le, cb + chunk);
     const int g = threadIdx.x / TB_GROUP, j = threadIdx.x % TB_GROUP;
-    int my = 0;
     const int gbase = (threadIdx.x & 31) & ~(TB_GROUP - 1);
+
+    // ---- count
+    int my = 0;
     for (int base = cb; base < ce; base += TB_NODES) {
         const int k = base + g;
         const bool valid = k < ce;
@@ -140,55 +176,46 @@ __global__ void __launch_bounds__(TB_THREADS) k_tree_count(int depth, const unsi
     }
     if (my) atomicAdd(&s_sum, my);
     __syncthreads();
-    if (threadIdx.x == 0) tb.blocksum[blockIdx.x] = s_sum;
-}
+    if (threadIdx.x == 0) tb_st_status(tb.bstat + (size_t)depth * G + blk, TB_PUBLISHED | (unsigned)s_sum);
 
-// Write phase: children of each node get contiguous indices after this depth.
-__global__ void __launch_bounds__(TB_THREADS) k_tree_write(int depth, const unsigned long long *__restrict__ keys,
-                                                           TreeBuf tb, int leaf)
-{
-    __shared__ int s_nch[TB_NODES];
-    __shared__ int s_excl[TB_NODES];
-    __shared__ int s_tot;
-    __shared__ int s_red[2][TB_THREADS / 32];
-    const int lb = tb.depth_beg[depth], le = tb.depth_beg[depth + 1];
-    const int G = gridDim.x;
-    // this block's first child index and the depth's child total, summed from
-    // the count phase's per-block sums (G of them, in block order; exact)
-    {
-        int before = 0, all = 0;
-        for (int i = threadIdx.x; i < G; i += TB_THREADS) {
-            const int v = tb.blocksum[i];
-            all += v;
-            if (i < (int)blockIdx.x) before += v;
-        }
-        before = __reduce_add_sync(0xffffffffu, before);
-        all = __reduce_add_sync(0xffffffffu, all);
-        if ((threadIdx.x & 31) == 0) { s_red[0][threadIdx.x >> 5] = before; s_red[1][threadIdx.x >> 5] = all; }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int bsum = 0, tsum = 0;
-            for (int w = 0; w < TB_THREADS / 32; w++) { bsum += s_red[0][w]; tsum += s_red[1][w]; }
-            long long nxt = (long long)le + tsum;
-            const bool over = nxt > tb.cap;
-            if (over) nxt = le;   // drop the level; the host reports the overflow
-            if (blockIdx.x == 0) {
-                if (over) atomicOr(tb.err, GG_EBIT_NODE_OVERFLOW);
-                tb.depth_beg[depth + 2] = (int)nxt;
-                tb.nnodes[0] = (int)nxt;
+    // ---- this block's first child index: the totals of the blocks before it
+    int before = 0;
+    for (int i = threadIdx.x; i < blk; i += TB_THREADS) {
+        const unsigned *w = tb.bstat + (size_t)depth * G + i;
+        unsigned v = tb_ld_status(w);
+        int spins = 0;
+        while (!(v & TB_PUBLISHED)) {
+            if (++spins > TB_SPIN_LIMIT) {
+                atomicOr(tb.err, GG_EBIT_SORT_TIMEOUT);
+                break;
             }
-            s_tot = over ? 0 : tsum;
-            s_red[0][0] = bsum;
+            __nanosleep(64);
+            v = tb_ld_status(w);
         }
-        __syncthreads();
+        before += (int)(v & ~TB_PUBLISHED);
     }
-    if (s_tot == 0) return;   // no children at all (or dropped on overflow)
-    const int nl = le - lb;
-    const int chunk = (nl + G - 1) / G;
-    const int cb = lb + blockIdx.x * chunk, ce = min(le, cb + chunk);
-    const int g = threadIdx.x / TB_GROUP, j = threadIdx.x % TB_GROUP;
-    int run = le + s_red[0][0];
-    __syncthreads();   // s_tot is reused below
+    before = __reduce_add_sync(0xffffffffu, before);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = before;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int off = 0;
+        for (int w = 0; w < TB_THREADS / 32; w++) off += s_red[w];
+        s_off = off;
+        if (blk == G - 1) {   // the last chunk: the depth's total is known
+            long long nxt = (long long)le + off + s_sum;
+            if (nxt > tb.cap) {
+                atomicOr(tb.err, GG_EBIT_NODE_OVERFLOW);
+                nxt = tb.cap;
+            }
+            tb.depth_beg[depth + 2] = (int)nxt;
+            tb.nnodes[0] = (int)nxt;
+        }
+    }
+    __syncthreads();   // also orders this block's count-phase stores before the reads below
+    if (s_sum == 0) return;
+
+    // ---- write
+    int run = le + s_off;
     for (int base = cb; base < ce; base += TB_NODES) {
         int k = base + g;
         bool valid = k < ce;
@@ -214,9 +241,10 @@ __global__ void __launch_bounds__(TB_THREADS) k_tree_write(int depth, const unsi
                     const int csz = chunk_size(e - s, leaf);
                     for (int c = j; c < nch; c += TB_GROUP) {
                         int idx = first + c;
+                        if (idx >= tb.cap) { atomicOr(tb.err, GG_EBIT_NODE_OVERFLOW); continue; }
                         int cs = s + c * csz, ce2 = min(e, cs + csz);
                         tb.start[idx] = cs; tb.end[idx] = ce2; tb.level[idx] = GG_CHUNK_LEVEL;
-                        tb.parent[idx] = k; tb.sys[idx] = sys; tb.counter[idx] = 0;
+                        tb.parent[idx] = k; tb.sys[idx] = sys;
                     }
                 } else {
                     int b = tb.bnd[(size_t)k * 8 + j];
@@ -229,9 +257,13 @@ __global__ void __launch_bounds__(TB_THREADS) k_tree_write(int depth, const unsi
                     }
                     if (bn > b) {
                         int idx = first + rank;
-                        tb.start[idx] = b; tb.end[idx] = bn;
-                        tb.level[idx] = common_level(keys[b], keys[bn - 1]);
-                        tb.parent[idx] = k; tb.sys[idx] = sys; tb.counter[idx] = 0;
+                        if (idx >= tb.cap) {
+                            atomicOr(tb.err, GG_EBIT_NODE_OVERFLOW);
+                        } else {
+                            tb.start[idx] = b; tb.end[idx] = bn;
+                            tb.level[idx] = common_level(keys[b], keys[bn - 1]);
+                            tb.parent[idx] = k; tb.sys[idx] = sys;
+                        }
                     }
                 }
             }
@@ -329,12 +361,11 @@ void gg_launch_tree(const unsigned long long *keys, const int *poff, int S, int 
     const int G = gg_tree_grid();
     k_tree_roots<<<(S + 127) / 128, 128, 0, st>>>(S, poff, tb);
     tb.cap = cap;
-    for (int depth = 0; depth < GG_MAX_DEPTH; depth++) {
-        k_tree_count<<<G, TB_THREADS, 0, st>>>(depth, keys, tb, leaf);
-        k_tree_write<<<G, TB_THREADS, 0, st>>>(depth, keys, tb, leaf);
-    }
+    cudaMemsetAsync(tb.ticket, 0, GG_MAX_DEPTH * sizeof(unsigned), st);
+    cudaMemsetAsync(tb.bstat, 0, (size_t)GG_MAX_DEPTH * G * sizeof(unsigned), st);
+    for (int depth = 0; depth < GG_MAX_DEPTH; depth++) k_tree_depth<<<G, TB_THREADS, 0, st>>>(depth, keys, tb, leaf);
     const int threads = 256, blocks = gg_num_sms() * 8;
     for (int depth = GG_MAX_DEPTH - 1; depth >= 0; depth--)
         k_tree_moments_depth<<<blocks, threads, 0, st>>>(depth, parts, dom, tb, nodes);
-    gg_note_launches(1 + 3 * GG_MAX_DEPTH);
+    gg_note_launches(1 + 2 * GG_MAX_DEPTH);
 }

@@ -6,12 +6,13 @@
 
 // per-node build arrays (device pointers), capacity `cap` nodes
 struct TreeBuf {
-    int *start, *end, *level, *parent, *sys, *nch, *child, *counter;
+    int *start, *end, *level, *parent, *sys, *nch, *child;
     int *bnd;          // 8 digit boundaries per node
     double *mass64;    // FP64 node mass (parent sums)
     int *depth_beg;    // GG_MAX_DEPTH + 2 entries
     int *nnodes;       // total nodes (device)
-    int *blocksum, *blockoff;
+    unsigned *bstat;   // per depth and block: published children totals (GG_MAX_DEPTH x grid)
+    unsigned *ticket;  // per depth: block tickets
     int cap;           // node capacity (set by gg_launch_tree)
     int *err;
 };
