@@ -790,14 +790,14 @@ def run_reference_arm_systems(args):
 
 
 # ---------------------------------------------------------------- one system per GPU
-def timed_steps(torch, stream, tree, walk, steps):
+def timed_steps(torch, stream, tree, walk, steps, build=None):
     """`steps` steps of build + walk between two CUDA events on the library's
     stream, with an event between build and walk.  Returns (total ms, mean
     build ms, mean walk ms)."""
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * steps + 1)]
     ev[0].record(stream)
     for k in range(steps):
-        tree.build()
+        (build or tree.build)()
         ev[2 * k + 1].record(stream)
         walk()
         ev[2 * k + 2].record(stream)
@@ -895,6 +895,16 @@ def run_system(args, torch, ggb200, dist, world, rank, local):
     torch.cuda.synchronize()
     if tree.last_stats()["error_word"]:
         raise RuntimeError("device error word %d" % tree.last_stats()["error_word"])
+    # a step of every target replays two CUDA graphs, the build's and the
+    # walk's launches, with an event between them; the same kernels, without
+    # the host issuing some 150 launches per step
+    graphs = act is None and not args.potential and not args.no_graph
+    if graphs:
+        tree.capture_step_parts(d_acc, d_pot, err_tol_force_acc=args.tol, err_tol_theta=0.0)
+        for _ in range(2):
+            tree.launch_step_part(0)
+            tree.launch_step_part(1)
+        torch.cuda.synchronize()
 
     clocks = ClockSampler(local)
     clocks.start()
@@ -903,7 +913,11 @@ def run_system(args, torch, ggb200, dist, world, rank, local):
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = ggb200.kernel_launches()
-    total_ms, build_ms, walk_ms = timed_steps(torch, stream, tree, walk, args.steps)
+    if graphs:
+        total_ms, build_ms, walk_ms = timed_steps(torch, stream, tree, lambda: tree.launch_step_part(1), args.steps,
+                                                  build=lambda: tree.launch_step_part(0))
+    else:
+        total_ms, build_ms, walk_ms = timed_steps(torch, stream, tree, walk, args.steps)
     if dist:
         dist.barrier()
     launches = ggb200.kernel_launches() - launches0
@@ -1086,7 +1100,8 @@ def run_system(args, torch, ggb200, dist, world, rank, local):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": name, "n": n, "active": na, "n_total": int(n_all), "err_tol_force_acc": args.tol,
                    "walk": "potential only (compute_potential)" if args.potential else "force and potential",
-                   "step": "extent+keys+sort+permute+tree+moments+relative walk (OldAcc on device)",
+                   "step": "extent+keys+sort+permute+tree+moments+relative walk (OldAcc on device)" +
+                           (", replayed as two CUDA graphs (build, walk)" if graphs else ""),
                    "l2": "inputs larger than L2 (32 B/particle records, %d MB + tree)" % (32 * n // 10 ** 6),
                    "leaf_size": kw["leaf_size"], "group_size": kw["group_size"], "flush": kw["flush"],
                    "blocks_per_sm": kw["blocks_per_sm"] or 2,
@@ -1166,6 +1181,7 @@ def main():
     ap.add_argument("--group-order", type=int, default=1, choices=[0, 1],
                     help="1: walk groups handed out most expensive first, by the previous walk's costs")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="issue the timed steps' launches one by one")
     ap.add_argument("--serve-window", type=float, default=2.0)
     # individual timesteps: the timed walk evaluates a seeded random fraction of
     # the particles (the tree is still built over all of them)

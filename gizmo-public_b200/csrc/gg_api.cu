@@ -54,9 +54,11 @@ struct DevBuf {
     T *p = nullptr;
     size_t cap = 0;
     const cudaStream_t *sref = nullptr;   // the owning context's current stream
+    long long *gen = nullptr;              // the owning context's count of buffer moves
     gg_status ensure(size_t n)
     {
         if (n <= cap && p) return GG_OK;
+        if (gen) ++*gen;   // a captured graph holding the old address is stale from here on
         const cudaStream_t s = sref ? *sref : (cudaStream_t)0;
         if (p) cudaFreeAsync(p, s);
         p = nullptr;
@@ -265,6 +267,12 @@ struct gg_ctx {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     int graph_launches = 0;               // kernels inside the captured step
+    // the same step captured as two graphs (0: build, 1: walk)
+    cudaGraph_t part_graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t part_exec[2] = {nullptr, nullptr};
+    int part_launches[2] = {0, 0};
+    // device buffers move when they grow: graphs captured before a move are refused
+    long long buf_gen = 0, graph_gen = -1, part_gen = -1;
     bool have_events = false;
     // host staging copies in flight: the next reuse of a staging buffer waits
     // for its own copy only
@@ -392,7 +400,7 @@ extern "C" gg_status gg_create(const gg_config *cfg, gg_ctx **out)
     cudaError_t e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete ctx; return gg_cuda_fail(e); }
     ctx->stream = ctx->own_stream;
-    ctx->for_each_buf([ctx](auto &b) { b.sref = &ctx->stream; });
+    ctx->for_each_buf([ctx](auto &b) { b.sref = &ctx->stream; b.gen = &ctx->buf_gen; });
     keep_pool_memory(ctx->device);
     if ((e = cudaEventCreateWithFlags(&ctx->stage_ev, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&ctx->vstage_ev, cudaEventDisableTiming)) != cudaSuccess ||
@@ -446,6 +454,10 @@ extern "C" gg_status gg_destroy(gg_ctx *c)
     if (c->stage_ev) cudaEventDestroy(c->stage_ev);
     if (c->vstage_ev) cudaEventDestroy(c->vstage_ev);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    for (int i = 0; i < 2; i++) {
+        if (c->part_exec[i]) cudaGraphExecDestroy(c->part_exec[i]);
+        if (c->part_graph[i]) cudaGraphDestroy(c->part_graph[i]);
+    }
     if (c->graph) cudaGraphDestroy(c->graph);
     if (c->have_events)
         for (int i = 0; i < 8; i++) cudaEventDestroy(c->ev[i]);
@@ -1058,25 +1070,88 @@ extern "C" gg_status gg_graph_capture_step(gg_ctx *c, double tol, double theta, 
     const int timing = c->cfg.timing;
     c->cfg.timing = 0;
     long long before = gg_kernel_launches();
+    const long long gen0 = c->buf_gen;
     GG_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     st = gg_build(c, nullptr);
     if (!st) st = run_walk(c, nullptr, 0, nullptr, tol, theta, d_acc, d_pot, nullptr);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(c->stream, &g);
     c->cfg.timing = timing;
+    if (!st && e == cudaSuccess && c->buf_gen != gen0) st = GG_ERR_NOT_BUILT;   // a buffer grew: step once uncaptured
     if (st) { if (g) cudaGraphDestroy(g); return st; }
     if (e != cudaSuccess) return gg_cuda_fail(e);
     c->graph_launches = (int)(gg_kernel_launches() - before);
     c->graph = g;
     e = cudaGraphInstantiate(&c->graph_exec, g, 0);
     if (e != cudaSuccess) { cudaGraphDestroy(g); c->graph = nullptr; c->graph_exec = nullptr; return gg_cuda_fail(e); }
+    c->graph_gen = c->buf_gen;
+    return GG_OK;
+}
+
+static void drop_part_graphs(gg_ctx *c)
+{
+    for (int i = 0; i < 2; i++) {
+        if (c->part_exec[i]) { cudaGraphExecDestroy(c->part_exec[i]); c->part_exec[i] = nullptr; }
+        if (c->part_graph[i]) { cudaGraphDestroy(c->part_graph[i]); c->part_graph[i] = nullptr; }
+    }
+    c->part_gen = -1;
+}
+
+extern "C" gg_status gg_graph_capture_parts(gg_ctx *c, double tol, double theta, double *d_acc, double *d_pot)
+{
+    if (!c || !d_acc || tol < 0 || theta < 0) return GG_ERR_INVALID;
+    if (!c->built) return GG_ERR_NOT_BUILT;
+    if (!c->stream) return GG_ERR_INVALID;   // the legacy default stream cannot be captured
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    drop_part_graphs(c);
+    if ((st = walk_setup(c))) return st;
+    if ((st = resolve_h_mixed(c))) return st;
+    const int timing = c->cfg.timing;
+    c->cfg.timing = 0;
+    const long long gen0 = c->buf_gen;
+    for (int part = 0; part < 2; part++) {
+        const long long before = gg_kernel_launches();
+        GG_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        st = part == 0 ? gg_build(c, nullptr) : run_walk(c, nullptr, 0, nullptr, tol, theta, d_acc, d_pot, nullptr);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        if (!st && e != cudaSuccess) st = gg_cuda_fail(e);
+        if (!st && c->buf_gen != gen0) st = GG_ERR_NOT_BUILT;   // a buffer grew: step once uncaptured
+        if (!st) {
+            c->part_graph[part] = g;
+            c->part_launches[part] = (int)(gg_kernel_launches() - before);
+            e = cudaGraphInstantiate(&c->part_exec[part], g, 0);
+            if (e != cudaSuccess) st = gg_cuda_fail(e);
+        } else if (g) {
+            cudaGraphDestroy(g);
+        }
+        if (st) {
+            c->cfg.timing = timing;
+            drop_part_graphs(c);
+            return st;
+        }
+    }
+    c->cfg.timing = timing;
+    c->part_gen = c->buf_gen;
+    return GG_OK;
+}
+
+extern "C" gg_status gg_graph_launch_part(gg_ctx *c, int32_t part)
+{
+    if (!c || part < 0 || part > 1) return GG_ERR_INVALID;
+    if (!c->part_exec[part] || c->part_gen != c->buf_gen) return GG_ERR_NOT_BUILT;
+    gg_status st;
+    if ((st = set_device(c))) return st;
+    GG_CUDA_TRY(cudaGraphLaunch(c->part_exec[part], c->stream));
+    gg_note_launches(c->part_launches[part]);
     return GG_OK;
 }
 
 extern "C" gg_status gg_graph_launch(gg_ctx *c)
 {
     if (!c) return GG_ERR_INVALID;
-    if (!c->graph_exec) return GG_ERR_NOT_BUILT;
+    if (!c->graph_exec || c->graph_gen != c->buf_gen) return GG_ERR_NOT_BUILT;
     gg_status st;
     if ((st = set_device(c))) return st;
     GG_CUDA_TRY(cudaGraphLaunch(c->graph_exec, c->stream));

@@ -138,6 +138,8 @@ def load_library():
             "gg_host_free": (i32, [P]),
             "gg_drift_systems": (i32, [P, P]),
             "gg_graph_capture_step": (i32, [P, dbl, dbl, P, P]),
+            "gg_graph_capture_parts": (i32, [P, dbl, dbl, P, P]),
+            "gg_graph_launch_part": (i32, [P, i32]),
             "gg_graph_launch": (i32, [P]),
             "gg_autotune": (i32, [P, dbl, dbl, ctypes.POINTER(Config), ctypes.POINTER(dbl)]),
             "gg_tune_accuracy": (i32, [P, dbl, dbl, ctypes.POINTER(Config), ctypes.POINTER(i32)]),
@@ -433,6 +435,15 @@ class GravityTree:
     def launch_step(self):
         """Replay the captured step on the context's stream (asynchronous)."""
         _check(self._lib.gg_graph_launch(self._h), "gg_graph_launch")
+
+    def capture_step_parts(self, d_acc, d_pot=None, err_tol_force_acc=0.0025, err_tol_theta=0.0):
+        """Capture the same step as two CUDA graphs, the build and the walk."""
+        _check(self._lib.gg_graph_capture_parts(self._h, err_tol_force_acc, err_tol_theta, _ptr(d_acc), _ptr(d_pot)),
+               "gg_graph_capture_parts")
+
+    def launch_step_part(self, part):
+        """Replay part 0 (build) or 1 (walk) of the captured step (asynchronous)."""
+        _check(self._lib.gg_graph_launch_part(self._h, part), "gg_graph_launch_part")
 
     def autotune(self, err_tol_force_acc=0.0025, err_tol_theta=0.0, d_active=None, n_active=0):
         """Pick leaf size, group size, blocks per SM, flush threshold and node

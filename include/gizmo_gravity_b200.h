@@ -274,11 +274,21 @@ gg_status gg_host_free(void *ptr);
  * be captured).  Run one uncaptured build + evaluation with the same systems
  * before capturing, so that every buffer is allocated.  A replay re-reads the
  * particles last loaded into the same buffers and keeps the relative
- * criterion's OldAcc on the device between replays.  Loading a system set of
- * a different total size invalidates the graph; capture again. */
+ * criterion's OldAcc on the device between replays.  A graph holds the
+ * device addresses of the context's buffers: once any of them has grown
+ * (another system set, another configuration, a stack retry), gg_graph_launch
+ * refuses the stale graph with GG_ERR_NOT_BUILT; capture again.  A capture
+ * during which a buffer had to grow is refused the same way (step once
+ * uncaptured first). */
 gg_status gg_graph_capture_step(gg_ctx *ctx, double err_tol_force_acc, double err_tol_theta, double *d_acc_out,
                                 double *d_pot_out);
 gg_status gg_graph_launch(gg_ctx *ctx);
+/* The same step captured as two graphs, part 0 the build and part 1 the walk,
+ * replayed one after the other by gg_graph_launch_part, so that a caller can
+ * time them apart with events between the launches.  Same rules as above. */
+gg_status gg_graph_capture_parts(gg_ctx *ctx, double err_tol_force_acc, double err_tol_theta, double *d_acc_out,
+                                 double *d_pot_out);
+gg_status gg_graph_launch_part(gg_ctx *ctx, int32_t part);
 /* Times the walk of the resident systems with the context's configuration
  * and over leaf size {8,16}, group size {32,64}, blocks per SM {2,3} and flush
  * threshold {64,128}, then the other node staging on the winner, each trial

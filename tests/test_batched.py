@@ -197,3 +197,44 @@ def test_autotune_for_an_active_subset():
     b50, b99, _ = ics.error_stats(base[rows], acc_d)
     t50, t99, _ = ics.error_stats(tuned[rows], acc_d)
     assert t99 <= 1.25 * b99 + 1e-5, (t99, b99)
+
+
+def test_two_part_graph_equals_uncaptured_steps_and_stale_graph_is_refused():
+    """The step captured as two graphs (build, walk) and replayed gives the
+    bits of the same steps issued launch by launch; after a buffer of the
+    context grows (a larger system set), the stale graphs are refused."""
+    import torch
+    ic = ics.clustered(120000, seed=95, n_clumps=20)
+    n = ic["pos"].shape[0]
+    rec = torch.from_numpy(ggb200.make_records(ic["pos"], ic["mass"], ic["h"]).view(np.uint8)).cuda()
+    res = []
+    for graphs in (False, True):
+        stream = torch.cuda.Stream()
+        with ggb200.GravityTree(group_size=64) as t:
+            t.set_stream(stream.cuda_stream)
+            t.load_device(rec, [n])
+            d_acc = torch.empty((n, 3), dtype=torch.float64, device="cuda")
+            d_pot = torch.empty(n, dtype=torch.float64, device="cuda")
+            t.build()
+            t.evaluate_device(d_acc, d_pot, err_tol_theta=0.7)
+            t.build()
+            t.evaluate_device(d_acc, d_pot, err_tol_force_acc=0.001)
+            if graphs:
+                t.capture_step_parts(d_acc, d_pot, err_tol_force_acc=0.001)
+            for _ in range(3):
+                if graphs:
+                    t.launch_step_part(0)
+                    t.launch_step_part(1)
+                else:
+                    t.build()
+                    t.evaluate_device(d_acc, d_pot, err_tol_force_acc=0.001)
+            stream.synchronize()
+            res.append((d_acc.cpu().numpy(), d_pot.cpu().numpy(), t.last_stats()["interactions"]))
+            if graphs:
+                big = torch.cat([rec, rec])
+                t.load_device(big, [n, n])
+                t.build()
+                with pytest.raises(ggb200.GravityError):
+                    t.launch_step_part(1)
+    (a0, p0, i0), (a1, p1, i1) = res
+    assert np.array_equal(a0, a1) and np.array_equal(p0, p1) and i0 == i1
