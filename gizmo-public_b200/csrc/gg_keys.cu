@@ -115,17 +115,23 @@ __global__ void k_extent_finalize(const unsigned long long *mm, int S, GGDomainD
     dom[s] = d;
 }
 
+// 21 levels: the top one from the one-level table, then ten steps of two
+// levels each from the two-level table (half the dependent table reads)
 __device__ __forceinline__ unsigned long long gg_ph_key21(unsigned x, unsigned y, unsigned z,
-                                                          const unsigned short *tab)
+                                                          const unsigned short *tab, const unsigned short *tab2)
 {
-    unsigned state = 0;
-    unsigned long long key = 0;
+    const int top = GG_MAX_LEVEL - 1;
+    unsigned pix = (((x >> top) & 1u) << 2) | (((y >> top) & 1u) << 1) | ((z >> top) & 1u);
+    unsigned e = tab[pix];   // state 0
+    unsigned long long key = e & 7u;
+    unsigned state = e >> 3;
 #pragma unroll
-    for (int lev = GG_MAX_LEVEL - 1; lev >= 0; --lev) {
-        unsigned pix = (((x >> lev) & 1u) << 2) | (((y >> lev) & 1u) << 1) | ((z >> lev) & 1u);
-        unsigned e = tab[state * 8 + pix];
-        key = (key << 3) | (e & 7u);
-        state = e >> 3;
+    for (int lev = top - 1; lev > 0; lev -= 2) {
+        const unsigned hi = (((x >> lev) & 1u) << 2) | (((y >> lev) & 1u) << 1) | ((z >> lev) & 1u);
+        const unsigned lo = (((x >> (lev - 1)) & 1u) << 2) | (((y >> (lev - 1)) & 1u) << 1) | ((z >> (lev - 1)) & 1u);
+        e = tab2[state * 64 + ((hi << 3) | lo)];
+        key = (key << 6) | (e & 63u);
+        state = e >> 6;
     }
     return key;
 }
@@ -134,8 +140,9 @@ __device__ __forceinline__ unsigned long long gg_ph_key21(unsigned x, unsigned y
 __global__ void k_keys(const GGPart *__restrict__ rec, int n, const int *__restrict__ poff, int S,
                        const GGDomainDev *__restrict__ dom, unsigned long long *keys, unsigned *vals, int *err)
 {
-    __shared__ unsigned short tab[GG_PH_NSTATES * 8];
+    __shared__ unsigned short tab[GG_PH_NSTATES * 8], tab2[GG_PH_NSTATES * 64];
     for (int i = threadIdx.x; i < GG_PH_NSTATES * 8; i += blockDim.x) tab[i] = GG_PH_TABLE_INIT[i];
+    for (int i = threadIdx.x; i < GG_PH_NSTATES * 64; i += blockDim.x) tab2[i] = GG_PH_TABLE2_INIT[i];
     __syncthreads();
     bool bad = false;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -150,7 +157,7 @@ __global__ void k_keys(const GGPart *__restrict__ rec, int n, const int *__restr
             unsigned long long u = (unsigned long long)__double_as_longlong(f);
             q[k] = (unsigned)((u & 0xFFFFFFFFFFFFFull) >> (52 - GG_MAX_LEVEL));
         }
-        keys[i] = gg_ph_key21(q[0], q[1], q[2], tab);
+        keys[i] = gg_ph_key21(q[0], q[1], q[2], tab, tab2);
         vals[i] = (unsigned)i;
     }
     if (bad) atomicOr(err, GG_EBIT_BAD_INPUT);
@@ -160,8 +167,9 @@ __global__ void k_keys(const GGPart *__restrict__ rec, int n, const int *__restr
 __global__ void k_keys_plain(const double *__restrict__ pos, long long n, GGDomainDev d, unsigned long long *keys,
                              int *err)
 {
-    __shared__ unsigned short tab[GG_PH_NSTATES * 8];
+    __shared__ unsigned short tab[GG_PH_NSTATES * 8], tab2[GG_PH_NSTATES * 64];
     for (int i = threadIdx.x; i < GG_PH_NSTATES * 8; i += blockDim.x) tab[i] = GG_PH_TABLE_INIT[i];
+    for (int i = threadIdx.x; i < GG_PH_NSTATES * 64; i += blockDim.x) tab2[i] = GG_PH_TABLE2_INIT[i];
     __syncthreads();
     bool bad = false;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -173,7 +181,7 @@ __global__ void k_keys_plain(const double *__restrict__ pos, long long n, GGDoma
             unsigned long long u = (unsigned long long)__double_as_longlong(f);
             q[k] = (unsigned)((u & 0xFFFFFFFFFFFFFull) >> (52 - GG_MAX_LEVEL));
         }
-        keys[i] = gg_ph_key21(q[0], q[1], q[2], tab);
+        keys[i] = gg_ph_key21(q[0], q[1], q[2], tab, tab2);
     }
     if (bad && err) atomicOr(err, GG_EBIT_BAD_INPUT);
 }

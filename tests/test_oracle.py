@@ -46,6 +46,7 @@ def test_key_generator_table_matches_oracle():
     """The packed state table used by the CUDA key kernel gives the oracle's keys."""
     import gen_ph_tables as g
     table = g.build_table()
+    table2 = g.build_table2(table)   # two levels per step, as the kernel walks it
     rng = np.random.default_rng(3)
     pos = rng.uniform(-5, 5, size=(3000, 3))
     d = oracle.find_extent(pos)
@@ -54,6 +55,7 @@ def test_key_generator_table_matches_oracle():
     for i in range(pos.shape[0]):
         q = [int(L.oracle_double_to_int(((pos[i, j] - d["corner"][j]) / d["len"]) + 1.0, 21)) for j in range(3)]
         assert g.key_python(q[0], q[1], q[2], 21, table) == (int(hi[i]) << 64 | int(lo[i]))
+        assert g.key_python2(q[0], q[1], q[2], 21, table, table2) == (int(hi[i]) << 64 | int(lo[i]))
 
 
 def test_direct_sum_conserves_momentum():
