@@ -1039,13 +1039,14 @@ def run_system(args, torch, ggb200, dist, world, rank, local):
     instrumented_tflops = (inter * FLOPS_PER_INTERACTION / (stages["ms_walk"] * 1e-3) / 1e12
                            if stages["ms_walk"] else None)
 
-    # HBM roofline of the sort (200 B per element: 8 passes x 24 B + 8 B histogram read)
+    # HBM roofline of the sort (268 B per element: 8 passes x 24 B + 8 B histogram read,
+    # + 68 B of the record gather in the last pass: 32 B read, 32 B written, 4 B rank)
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         hbm_peak, hbm_src = float(peaks["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
     except Exception:
         hbm_peak, hbm_src = 6650.0, "fallback 6.65 TB/s"
-    sort_gbs = 200.0 * n / (stages["ms_sort"] * 1e-3) / 1e9 if stages["ms_sort"] else None
+    sort_gbs = 268.0 * n / (stages["ms_sort"] * 1e-3) / 1e9 if stages["ms_sort"] else None
 
     # end to end through the public API with host buffers
     e2e = None
@@ -1123,7 +1124,7 @@ def run_system(args, torch, ggb200, dist, world, rank, local):
                      "peak_source": "measured FP32 FMA probe (gg_fp32_peak_probe) on this GPU",
                      "walk_ms": walk_ms, "instrumented_step_achieved": instrumented_tflops},
         "roofline_sort": {"bound": "hbm", "achieved": sort_gbs, "peak": hbm_peak, "unit": "GB/s",
-                          "frac": (sort_gbs / hbm_peak) if sort_gbs else None, "bytes_per_element": 200,
+                          "frac": (sort_gbs / hbm_peak) if sort_gbs else None, "bytes_per_element": 268,
                           "peak_source": hbm_src},
         "clocks": clk, "gpu_launches": int(launches), "e2e": e2e, "cpu_baseline": cpu,
     }

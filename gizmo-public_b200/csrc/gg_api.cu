@@ -658,13 +658,16 @@ extern "C" gg_status gg_build(gg_ctx *c, const gg_domain *domains)
     }
     if (N > 0) gg_launch_keys(c->in_rec.p, N, c->poff.p, S, c->dom.p, c->keys.p, c->perm.p, c->err.p, s);
     if (timing) cudaEventRecord(c->ev[1], s);
+    // the sort's last pass also moves the records into key order
+    bool gathered = false;
     if (N > 1) {
+        const SortGather g = {c->in_rec.p, c->part.p, c->rank.p};
         st = gg_sort_pairs_run(c->keys.p, c->perm.p, N, 3 * GG_MAX_LEVEL, sbits, c->poff.p, S, c->sort_scratch.p,
-                               c->err.p, s);
+                               c->err.p, s, &g, &gathered);
         if (st) return st;
     }
+    if (N > 0 && !gathered) gg_launch_permute(c->perm.p, c->in_rec.p, c->part.p, c->rank.p, N, s);
     if (timing) cudaEventRecord(c->ev[2], s);
-    if (N > 0) gg_launch_permute(c->perm.p, c->in_rec.p, c->part.p, c->rank.p, N, s);
     gg_launch_tree(c->keys.p, c->poff.p, S, c->cfg.leaf_size, c->ncap, tree_buf(c), c->part.p, c->dom.p, c->nodes.p, s);
     if (timing) cudaEventRecord(c->ev[3], s);
     GG_CUDA_TRY(cudaGetLastError());

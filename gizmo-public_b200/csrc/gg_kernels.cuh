@@ -26,8 +26,18 @@ void gg_launch_keys_plain(const double *pos, long long n, const GGDomainDev &d, 
 
 size_t gg_sort_scratch_bytes(long long n);
 int gg_sort_bits();
+// Records moved by the last pass of a sort whose values are record indices:
+// out[position] = in[value], rank[value] = position.
+struct SortGather {
+    const GGPart *in;
+    GGPart *out;
+    unsigned *rank;
+};
+// gather (nullable): done by the last pass; *gathered says whether it was (no
+// pass runs for n <= 1 or no bits).
 gg_status gg_sort_pairs_run(unsigned long long *keys, unsigned *vals, long long n, int key_bits, int sys_bits,
-                            const int *poff, int S, void *scratch, int *err, cudaStream_t st);
+                            const int *poff, int S, void *scratch, int *err, cudaStream_t st,
+                            const SortGather *gather = nullptr, bool *gathered = nullptr);
 
 void gg_launch_permute(const unsigned *perm, const GGPart *in, GGPart *out, unsigned *rank, int n, cudaStream_t st);
 int gg_tree_grid();

@@ -157,11 +157,15 @@ struct SortSmem {
 
 // one pass: digit = (key >> shift) & (RADIX-1), or of the system id when sys_mode.
 // status: this pass's look-back words; status_next: the next pass's, of which
-// this tile clears its own (nullptr for the last pass)
+// this tile clears its own (nullptr for the last pass).  GATHER (the last pass
+// of a build's sort): each pair's value is a record index, and the pass also
+// moves that record to the pair's sorted position and records the position.
+template <bool GATHER>
 __global__ void __launch_bounds__(SORT_THREADS, GG_SORT_MINB) k_sort_pass(
     const unsigned long long *__restrict__ kin, const unsigned *__restrict__ vin, unsigned long long *__restrict__ kout,
     unsigned *__restrict__ vout, int n, int shift, int sys_mode, const int *__restrict__ poff, int S,
-    const unsigned *__restrict__ g_off, unsigned *status, unsigned *status_next, unsigned *tile_counter, int *err)
+    const unsigned *__restrict__ g_off, unsigned *status, unsigned *status_next, unsigned *tile_counter, int *err,
+    SortGather gather)
 {
     extern __shared__ __align__(16) unsigned char sort_smem_raw[];
     SortSmem &sm = *reinterpret_cast<SortSmem *>(sort_smem_raw);
@@ -311,8 +315,17 @@ __global__ void __launch_bounds__(SORT_THREADS, GG_SORT_MINB) k_sort_pass(
         const unsigned dd = sm.dig[i];
         const unsigned gpos = sm.gbase[dd] + (unsigned)i - sm.texcl[dd];
         if (gpos < (unsigned)n) {   // always true unless a look-back gave up
+            const unsigned v = sm.vals[i];
             kout[gpos] = sm.keys[i];
-            vout[gpos] = sm.vals[i];
+            vout[gpos] = v;
+            if (GATHER) {
+                const unsigned src = v < (unsigned)n ? v : 0u;   // only after a failed sort, which is reported
+                const int4 *from = reinterpret_cast<const int4 *>(gather.in + src);
+                int4 *to = reinterpret_cast<int4 *>(gather.out + gpos);
+                to[0] = __ldg(from);
+                to[1] = __ldg(from + 1);
+                gather.rank[src] = gpos;
+            }
         }
     }
 }
@@ -341,8 +354,10 @@ static int sort_smem_bytes() { return (int)sizeof(SortSmem); }
 // gg_sort_scratch_bytes(n) bytes, 256-byte aligned.  The
 // result is left in keys/vals.
 gg_status gg_sort_pairs_run(unsigned long long *keys, unsigned *vals, long long n, int key_bits, int sys_bits,
-                            const int *poff, int S, void *scratch, int *err, cudaStream_t st)
+                            const int *poff, int S, void *scratch, int *err, cudaStream_t st,
+                            const SortGather *gather, bool *gathered)
 {
+    if (gathered) *gathered = false;
     const int nkey = sort_passes(key_bits), nsys = sort_passes(sys_bits), np = nkey + nsys;
     if (np <= 0 || n <= 1) return GG_OK;
     if (np > GG_SORT_MAX_PASSES || n >= (1ll << 30)) return GG_ERR_TOO_LARGE;
@@ -374,15 +389,25 @@ gg_status gg_sort_pairs_run(unsigned long long *keys, unsigned *vals, long long 
         gg_note_launches(2);
     }
     // the attribute is per device: set it on every call (cheap)
-    GG_CUDA_TRY(cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, sort_smem_bytes()));
+    GG_CUDA_TRY(cudaFuncSetAttribute(k_sort_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sort_smem_bytes()));
+    if (gather) {
+        GG_CUDA_TRY(cudaFuncSetAttribute(k_sort_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         sort_smem_bytes()));
+    }
+    const SortGather none = {nullptr, nullptr, nullptr};
     unsigned long long *ka = keys, *kb = kalt;
     unsigned *va = vals, *vb = valt;
     for (int pass = 0; pass < np; pass++) {
         const int sys_mode = pass >= nkey;
         const int shift = sys_mode ? SORT_BITS * (pass - nkey) : SORT_BITS * pass;
-        k_sort_pass<<<(unsigned)ntiles, SORT_THREADS, sort_smem_bytes(), st>>>(
-            ka, va, kb, vb, (int)n, shift, sys_mode, poff, S, off + pass * RADIX, status[pass & 1],
-            pass + 1 < np ? status[(pass + 1) & 1] : nullptr, counters + pass, err);
+        if (gather && pass == np - 1)
+            k_sort_pass<true><<<(unsigned)ntiles, SORT_THREADS, sort_smem_bytes(), st>>>(
+                ka, va, kb, vb, (int)n, shift, sys_mode, poff, S, off + pass * RADIX, status[pass & 1], nullptr,
+                counters + pass, err, *gather);
+        else
+            k_sort_pass<false><<<(unsigned)ntiles, SORT_THREADS, sort_smem_bytes(), st>>>(
+                ka, va, kb, vb, (int)n, shift, sys_mode, poff, S, off + pass * RADIX, status[pass & 1],
+                pass + 1 < np ? status[(pass + 1) & 1] : nullptr, counters + pass, err, none);
         gg_note_launches(1);
         unsigned long long *tk = ka; ka = kb; kb = tk;
         unsigned *tv = va; va = vb; vb = tv;
@@ -391,6 +416,7 @@ gg_status gg_sort_pairs_run(unsigned long long *keys, unsigned *vals, long long 
         GG_CUDA_TRY(cudaMemcpyAsync(keys, ka, (size_t)n * 8, cudaMemcpyDeviceToDevice, st));
         GG_CUDA_TRY(cudaMemcpyAsync(vals, va, (size_t)n * 4, cudaMemcpyDeviceToDevice, st));
     }
+    if (gathered) *gathered = gather != nullptr;
     return GG_OK;
 }
 
@@ -419,9 +445,10 @@ gg_status gg_sort_timeout_selftest(cudaStream_t st)
     cudaMemsetAsync(base, 0, (size_t)(p - base), st);
     const unsigned one = 1;   // the CTA takes tile 1; tile 0 is never started
     cudaMemcpyAsync(counter, &one, sizeof one, cudaMemcpyHostToDevice, st);
-    cudaFuncSetAttribute(k_sort_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, sort_smem_bytes());
-    k_sort_pass<<<1, SORT_THREADS, sort_smem_bytes(), st>>>(kin, vin, kout, vout, n, 0, 0, nullptr, 1, off, status,
-                                                             nullptr, counter, err);
+    cudaFuncSetAttribute(k_sort_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sort_smem_bytes());
+    const SortGather none = {nullptr, nullptr, nullptr};
+    k_sort_pass<false><<<1, SORT_THREADS, sort_smem_bytes(), st>>>(kin, vin, kout, vout, n, 0, 0, nullptr, 1, off, status,
+                                                             nullptr, counter, err, none);
     gg_note_launches(1);
     int herr = 0;
     cudaError_t e = cudaGetLastError();

@@ -95,8 +95,8 @@ typedef struct gg_stats {
     int32_t n_groups;       /* walk groups */
     int32_t error_word;     /* device error bits of the last call */
     double ms_keys;         /* extent + keys (device time, when timing is on) */
-    double ms_sort;
-    double ms_build;        /* permute + tree + moments */
+    double ms_sort;         /* key sort, whose last pass also moves the records into key order */
+    double ms_build;        /* tree + moments */
     double ms_walk;
     int64_t far_entries;    /* interaction-list entries evaluated without softening (all groups) */
     int64_t near_entries;   /* entries that needed the softening branch */
