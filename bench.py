@@ -547,7 +547,7 @@ def run_ensemble(args, torch, ggb200, dist, world, rank, local):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": ENSEMBLE_NAME, "n_systems": S, "n": n, "n_total": int(n_all),
                    "err_tol_force_acc": tol, "tuned": tuned, "autotune_walk_ms": tuned_ms, "autotune_s": t_tune,
-                   "step": "one CUDA graph: extent+keys+sort+permute+tree+moments+relative walk of every system",
+                   "step": "one CUDA graph: extent+keys+sort+record gather+tree+moments+relative walk of every system",
                    "l2": "inputs larger than L2 (1.5 GB of records)",
                    "parallelism": "independent ensemble per GPU" if world > 1 else "1 GPU"},
         "batched_vs_plain": {"graph_ms": ms_step, "batched_uncaptured_ms": plain_batched_ms, "plain_ms": plain_ms,
@@ -741,7 +741,7 @@ def run_split(args, torch, ggb200, dist, world, rank, local):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": name, "n": n, "share": share, "err_tol_force_acc": args.tol,
-                   "step": "all-gather of 32-byte records + extent+keys+sort+permute+tree+moments on every rank + "
+                   "step": "all-gather of 32-byte records + extent+keys+sort+record gather+tree+moments on every rank + "
                            "relative walk of the rank's own particles",
                    "parallelism": "one system over %d GPUs" % world},
         "interactions_per_particle_rank0": st["interactions"] / max(share[rank], 1),
@@ -829,7 +829,7 @@ def reference_errors(ref, acc_dir, pot_dir, mass, acc_gpu, pot_gpu):
 
 def run_system(args, torch, ggb200, dist, world, rank, local):
     """One system per GPU (independent seeded systems per rank: weak scaling).
-    A step = build (extent, keys, sort, permute, tree, moments) + relative walk
+    A step = build (extent, keys, sort with the record gather, tree, moments) + relative walk
     of every particle, OldAcc left on the device by the previous step.  With
     --subset-frac (default 0.1 on the clustered system) a second timed loop
     walks a seeded random subset of targets on a full rebuild (individual
@@ -1101,7 +1101,7 @@ def run_system(args, torch, ggb200, dist, world, rank, local):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": name, "n": n, "active": na, "n_total": int(n_all), "err_tol_force_acc": args.tol,
                    "walk": "potential only (compute_potential)" if args.potential else "force and potential",
-                   "step": "extent+keys+sort+permute+tree+moments+relative walk (OldAcc on device)" +
+                   "step": "extent+keys+sort+record gather+tree+moments+relative walk (OldAcc on device)" +
                            (", replayed as two CUDA graphs (build, walk)" if graphs else ""),
                    "l2": "inputs larger than L2 (32 B/particle records, %d MB + tree)" % (32 * n // 10 ** 6),
                    "leaf_size": kw["leaf_size"], "group_size": kw["group_size"], "flush": kw["flush"],
